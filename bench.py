@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Throughput of the fixed-charge nonbonded energy + force evaluation (TIP3P water boxes).
+
+A step is one energy + force evaluation of one periodic water box: cluster-pair
+neighbour build, fused real-space LJ + erfc-Coulomb with exclusion correction, PME
+(spread, FFT, influence function, FFT, gather), forces back in caller order.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload water3000|water216|water100k] [--precision mixed|fp64]
+
+Multi-GPU (torchrun, one rank per GPU): each rank evaluates its own replica box (seeded
+per rank); no data-path collective exists for one system, so the run is weak scaling
+over independent replicas. `--impl reference` times the CPU restatement of the
+reference's pure-torch algorithm (O(N^2) neighbour list, pair terms, PME) on the host
+cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(REPO, "torchff-lib_b200"), REPO):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "3000-water PME energy+force evals/s"
+WORKLOAD_TEXT = {
+    "water3000": "3000 rigid TIP3P waters (9000 atoms), cubic L=4.482 nm, rc=1.0 nm, Ewald alpha 2.628 nm^-1, "
+                 "PME 48^3 order 6, LJ on O, intramolecular pairs excluded",
+    "water216": "216 rigid TIP3P waters (648 atoms), cubic L=1.8662 nm, rc=0.9 nm, Ewald alpha 2.920 nm^-1, "
+                "PME 20^3 order 6",
+    "water100k": "100,000 rigid TIP3P waters (300,000 atoms), cubic L=14.42 nm, rc=1.0 nm, PME 144^3 order 6",
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=list(WORKLOAD_TEXT), default="water3000")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def water_box(name: str, seed: int):
+    from torchff_b200 import water as W
+
+    return {"water3000": W.water_box_3000, "water216": W.water_box_216, "water100k": W.water_box_100k}[name](seed)
+
+
+# ---------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        self.t0 = time.time()
+
+    def stop(self):
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------------------
+
+def count_pairs(wb, dtype, device):
+    """In-cutoff half pairs (exclusions removed) of the frame: the algorithmic pair count."""
+    import torch
+
+    import torchff_b200  # noqa: F401
+    from torchff_b200.nblist import convert_pairs_coo_to_csr
+
+    rp, col = (t.to(device) for t in convert_pairs_coo_to_csr(torch.tensor(wb.nblist_exclusions), wb.natoms))
+    x = torch.tensor(wb.coords, dtype=torch.float64, device=device)
+    b = torch.tensor(wb.box, dtype=torch.float64, device=device)
+    cap = int(wb.natoms * 4 / 3 * math.pi * wb.cutoff ** 3 * 100 / 2 * 1.5)
+    _, n = torch.ops.torchff.build_neighbor_list_cell_list(x, b, wb.cutoff, cap, rp, col, False)
+    return int(n.item())
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def ncu_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch from the committed ncu summary, if one exists."""
+    path = os.path.join(REPO, "profiles", "ncu_traffic.txt")
+    try:
+        with open(path) as f:
+            for ln in f:
+                p = ln.split()
+                if len(p) >= 3 and p[0] == kernel and p[1] == workload:
+                    return float(p[2])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline_sample(wb, evals: int = 2) -> dict:
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    for _ in range(evals):
+        O.fixed_charge_energy(wb.coords, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
+                              wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
+                              138.935456)
+    dt = time.perf_counter() - t0
+    return {"value": evals / dt, "unit": "evals/s", "cores": 1, "kind": "port",
+            "sample": f"{evals} full evaluations of the same box by the numpy oracle (O(N^2) neighbour list, "
+                      f"pair terms, PME with analytic forces), one thread"}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}; launch N>1 with torch.distributed.run")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+
+    import torchff_b200  # noqa: F401
+    from torchff_b200.system import FixedChargeSystem, StageTimer
+
+    dtype = torch.float32 if args.precision == "mixed" else torch.float64
+    wb = water_box(args.workload, seed=rank)
+    system = FixedChargeSystem.from_water_box(wb, dtype=dtype, device=device)
+    x = torch.tensor(wb.coords, dtype=dtype, device=device)
+    b = torch.tensor(wb.box, dtype=dtype, device=device)
+    energy = torch.empty(1, dtype=torch.float64, device=device)
+    forces = torch.empty_like(x)
+    timer = StageTimer()
+
+    # capture one evaluation (with its stage events) in a CUDA graph
+    side = torch.cuda.Stream(device)
+    side.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            system.evaluate_timed_into(x, b, energy, forces, timer)
+    torch.cuda.current_stream(device).wait_stream(side)
+    torch.cuda.synchronize(device)
+    if system.status() != 0:
+        raise RuntimeError("cluster neighbour list overflow")
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        system.evaluate_timed_into(x, b, energy, forces, timer)
+
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)   # > 126 MB L2
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i in range(args.warmup):
+        flush.fill_(i & 0xff)
+        graph.replay()
+    torch.cuda.synchronize(device)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    step_ms, tile_ms, stage_acc = [], [], {k: 0.0 for k in StageTimer.STAGES}
+    for i in range(args.steps):
+        flush.fill_(i & 0xff)
+        start.record()
+        graph.replay()
+        end.record()
+        end.synchronize()
+        step_ms.append(start.elapsed_time(end))
+        st = timer.stages_ms()
+        tile_ms.append(st["tile_kernel"])
+        for k, v in st.items():
+            stage_acc[k] += v
+    torch.cuda.synchronize(device)
+    if world > 1:
+        dist.barrier()
+    clocks.stop()
+    total_ms = sum(step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * args.steps / (max_ms / 1e3)
+
+    # end to end through the C ABI with host buffers (H2D coords+box, eval, D2H forces+energy)
+    hx = torch.tensor(wb.coords, dtype=torch.float64).pin_memory()
+    hb = torch.tensor(wb.box, dtype=torch.float64).pin_memory()
+    hf = torch.empty((wb.natoms, 3), dtype=torch.float64).pin_memory()
+    for i in range(5):
+        system.evaluate_host(hx, hb, hf)
+    e2e_ms = []
+    if world > 1:
+        dist.barrier()
+    for i in range(args.e2e_steps):
+        flush.fill_(i & 0xff)
+        start.record()
+        system.evaluate_host(hx, hb, hf)
+        end.record()
+        end.synchronize()
+        e2e_ms.append(start.elapsed_time(end))
+    te = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.e2e_steps / (float(te.item()) / 1e3)
+    h2d = wb.natoms * 3 * 8 + 9 * 8
+    d2h = wb.natoms * 3 * 8 + 8
+
+    result = None
+    if rank == 0:
+        npairs = count_pairs(wb, dtype, device)
+        peaks = measured_peaks()
+        sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+        fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12        # TFLOP/s, FMA = 2 flops
+        tile_mean_ms = statistics.mean(tile_ms)
+        flops = 60.0 * npairs                                   # algorithmic flops per launch
+        achieved = flops / (tile_mean_ms * 1e-3) / 1e12
+        stages = {k: round(v / args.steps * 1e3, 3) for k, v in stage_acc.items()}
+        clk = clocks.summary()
+        result = {
+            "metric": METRIC if args.workload == "water3000" else f"{args.workload} PME energy+force evals/s",
+            "value": round(value, 2),
+            "unit": "evals/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(max_ms / args.steps, 5),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32" if dtype == torch.float32 else "f64",
+            "data": "synthetic (seeded TIP3P lattice box, one replica per rank)",
+            "config": {
+                "workload": f"{args.workload}: {WORKLOAD_TEXT[args.workload]}",
+                "precision": "mixed: FP32 pair/spline arithmetic, int64 fixed-point forces, FP64 energies"
+                if dtype == torch.float32 else "fp64",
+                "path": "FixedChargeSystem (cluster-pair build + fused real-space tile kernel + PME), "
+                        "one CUDA-graph replay per step",
+                "l2": "flushed between timed steps (256 MiB device write)",
+                "parallelism": f"replicas x{world}",
+                "stage_us_mean": stages,
+            },
+            "e2e": {"value": round(e2e_value, 2), "unit": "evals/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "path": "tff_system_eval_host (C ABI): pinned host coords/box -> device -> host forces"},
+            "gpu_launches": system.kernel_launches() * args.steps,
+            "roofline": {
+                "kernel": "tile_kernel<float> (fused real-space LJ + erfc Coulomb, 32x32 cluster tiles)",
+                "bound": "fp32",
+                "achieved": round(achieved, 4),
+                "peak": round(fp32_peak, 2),
+                "unit": "TFLOP/s",
+                "frac": round(achieved / fp32_peak, 5),
+                "traffic": ncu_traffic("tile_kernel", args.workload),
+                "algorithmic": f"60 flop x {npairs} in-cutoff pairs per launch / mean tile-kernel time "
+                               f"{tile_mean_ms * 1e3:.2f} us (CUDA events in the graph)",
+                "peak_source": f"FP32 nominal 148 SM x 128 lanes x 2 flop x {sm_max:.0f} MHz (sm_max_mhz of "
+                               "MEASURED_PEAKS.json; no measured FP32 peak exists)",
+            },
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline_sample(wb)
+    del graph
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+# reference arm: the CPU restatement of the reference's pure-torch path
+# ---------------------------------------------------------------------------------------
+
+def _ref_worker_init():
+    for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[v] = "1"
+
+
+def _ref_eval(task):
+    workload, seed = task
+    from oracle import oracle as O
+
+    wb = water_box(workload, seed)
+    t0 = time.perf_counter()
+    O.fixed_charge_energy(wb.coords, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
+                          wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid, 138.935456)
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    if args.workload == "water100k":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference CPU path keeps an O(N^2) all-pairs "
+                          "buffer (~720 GB at 300,000 atoms); not run"}))
+        return
+    workers = max(1, min(os.cpu_count() or 1, 16, max(args.steps, 1)))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers, initializer=_ref_worker_init) as pool:
+        pool.map(_ref_eval, [(args.workload, 1000 + i) for i in range(max(args.warmup, workers))])
+        t0 = time.perf_counter()
+        per = pool.map(_ref_eval, [(args.workload, i) for i in range(args.steps)])
+        wall = time.perf_counter() - t0
+    value = args.steps / wall
+    line = {
+        "impl": "reference",
+        "metric": METRIC if args.workload == "water3000" else f"{args.workload} PME energy+force evals/s",
+        "value": round(value, 4),
+        "unit": "evals/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(statistics.mean(per) * 1e3, 2),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded TIP3P lattice boxes)",
+        "config": {"workload": f"{args.workload}: {WORKLOAD_TEXT[args.workload]}",
+                   "path": "numpy restatement of the reference pure-torch path (O(N^2) pair search, LJ type "
+                           "tables, real-space Ewald with exclusion correction, PME), analytic forces",
+                   "parallelism": f"{workers} host processes, one evaluation each at a time"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "evals/s", "cores": workers, "kind": "port",
+                         "sample": f"{args.steps} full evaluations spread over {workers} single-thread processes"},
+        "e2e": {"value": round(value, 4), "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,232 @@
+/*
+ * tffb200.h -- C ABI of libtffb200.so, the sm_100a implementation of torchff's
+ * fixed-charge nonbonded energy/force path (neighbour list, real-space Coulomb /
+ * Lennard-Jones / Ewald pair terms, rank-0 PME).
+ *
+ * Conventions shared by every entry point
+ *   - All array arguments are DEVICE pointers (the *_host functions excepted).
+ *   - `dtype` selects the arithmetic: TFF_F32 = mixed precision (FP32 pair and spline
+ *     arithmetic, 64-bit fixed-point force/grid accumulation, FP64 energies; results are
+ *     bit-identical run to run), TFF_F64 = float64 throughout (FP64 atomics).
+ *     Floating-point arrays are float* for TFF_F32 and double* for TFF_F64.
+ *   - Coordinates are (N, 3) row-major; `box` is a (3, 3) row-major matrix whose rows
+ *     are the box vectors (torchff/pbc.py), or NULL for an open system where allowed.
+ *   - Index arrays are int64, pairs are (P, 2) row-major; a pair holding -1 is skipped.
+ *   - Energies are written, gradients (dE/dx, dE/dq, ...) are written (not accumulated).
+ *     A NULL gradient pointer skips that gradient.
+ *   - Scratch memory is passed in by the caller as `workspace` of at least the size the
+ *     matching *_workspace_bytes() reports; the library itself never calls cudaMalloc in
+ *     these entry points (PME plans and system objects own their memory, see below).
+ *   - Work is enqueued on `stream` (a cudaStream_t); nothing synchronises with the host
+ *     except the *_host entry points. Every call can be captured in a CUDA graph.
+ *   - Return value: TFF_OK or an error code; tff_last_error() describes the last error
+ *     of the calling thread.
+ */
+#ifndef TFFB200_H
+#define TFFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *tff_stream_t; /* identical to cudaStream_t */
+
+enum tff_dtype { TFF_F32 = 0, TFF_F64 = 1 };
+
+enum tff_status {
+  TFF_OK = 0,
+  TFF_ERR_INVALID = 1,     /* bad argument (shape, dtype, NULL, unsupported box) */
+  TFF_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  TFF_ERR_CUFFT = 3,       /* a cuFFT call failed */
+  TFF_ERR_WORKSPACE = 4,   /* workspace too small */
+  TFF_ERR_CAPACITY = 5     /* a fixed-capacity list overflowed (see tff_system_status) */
+};
+
+int tff_version(void);
+const char *tff_last_error(void);
+/* Number of SMs the kernels size their grids for on the current device. */
+int tff_device_sm_count(void);
+
+/* ------------------------------------------------------------------------------
+ * Neighbour lists
+ * --------------------------------------------------------------------------- */
+
+/* Replaces torch.ops.torchff.build_neighbor_list_nsquared / _out
+ * (csrc/nblist/nblist_interface.cpp:5-6, csrc/nblist/nblist_nsquared_cuda.cu:129-199).
+ * All pairs (i, j), i > j (i == j too when include_self), with |r_ij| <= cutoff under the
+ * minimum image of `box` (NULL = open boundaries), skipping pairs listed in the symmetric
+ * CSR exclusion structure (excl_row_ptr (N+1), excl_col; both NULL = none).
+ * `pairs` (max_npairs, 2) is filled with -1 and the first min(found, max_npairs) rows
+ * receive pairs; *npairs (device int32) receives the number FOUND, which may exceed
+ * max_npairs (overflow). In TFF_F32 mode pairs within 1e-5 relative of the cutoff are
+ * re-tested in FP64, so the pair set equals the FP64 one. Needs no workspace. */
+int tff_nblist_nsquared(int dtype, int64_t natoms, const void *coords, const void *box,
+                        double cutoff, const int64_t *excl_row_ptr, const int64_t *excl_col,
+                        int include_self, int64_t *pairs, int64_t max_npairs, int32_t *npairs,
+                        tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.build_neighbor_list_cell_list / _out
+ * (csrc/nblist/nblist_interface.cpp:7-8, csrc/nblist/nblist_clist_cuda.cu:367-525).
+ * Same output contract as tff_nblist_nsquared; requires an orthorhombic `box`. Atoms are
+ * binned on a Morton-ordered cell grid, grouped in 32-atom clusters and cluster pairs are
+ * screened by bounding boxes before a 32x32 warp tile test.
+ * max_cluster_neighbors: capacity of each cluster's neighbour-cluster list (0 = default). */
+size_t tff_nblist_cell_list_workspace_bytes(int dtype, int64_t natoms, int max_cluster_neighbors);
+int tff_nblist_cell_list(int dtype, int64_t natoms, const void *coords, const void *box,
+                         double cutoff, const int64_t *excl_row_ptr, const int64_t *excl_col,
+                         int include_self, int64_t *pairs, int64_t max_npairs, int32_t *npairs,
+                         int max_cluster_neighbors, void *workspace, size_t workspace_bytes,
+                         tff_stream_t stream);
+
+/* ------------------------------------------------------------------------------
+ * Pair terms over an explicit pair list
+ * --------------------------------------------------------------------------- */
+
+/* Workspace of every *_atom_pairs entry point; ntypes = size of the LJ type table
+ * (0 when type tables are not used). */
+size_t tff_pairs_workspace_bytes(int dtype, int64_t natoms, int64_t ntypes);
+
+/* Replaces torch.ops.torchff.compute_nonbonded_energy_from_atom_pairs
+ * (csrc/nonbonded/nonbonded_interface.cpp:9, csrc/nonbonded/nonbonded_atom_pairs_cuda.cu:17-141, 144-238).
+ * E = sum_{r<=rc} k q_i q_j (1/r - [do_shift]/rc) + 4 eps_ij ((s_ij/r)^12 - (s_ij/r)^6),
+ * s_ij = (s_i+s_j)/2, eps_ij = sqrt(eps_i eps_j). Gradients: dE/dx (N,3), dE/dsigma (N),
+ * dE/depsilon (N; pairs with eps_ij = 0 contribute 0), dE/dq (N). */
+int tff_nonbonded_atom_pairs(int dtype, int64_t natoms, const void *coords, int64_t npairs,
+                             const int64_t *pairs, const void *box, const void *sigma,
+                             const void *epsilon, const void *charges, double coul_constant,
+                             double cutoff, int do_shift, void *energy, void *grad_coords,
+                             void *grad_sigma, void *grad_epsilon, void *grad_charges,
+                             void *workspace, size_t workspace_bytes, tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.compute_nonbonded_forces_from_atom_pairs
+ * (csrc/nonbonded/nonbonded_interface.cpp:10, csrc/nonbonded/nonbonded_atom_pairs_cuda.cu:263-305):
+ * ADDS the shifted Coulomb + LJ forces -dE/dx into `forces` (N,3). */
+int tff_nonbonded_forces_atom_pairs(int dtype, int64_t natoms, const void *coords,
+                                    int64_t npairs, const int64_t *pairs, const void *box,
+                                    const void *sigma, const void *epsilon, const void *charges,
+                                    double coul_constant, double cutoff, void *forces,
+                                    void *workspace, size_t workspace_bytes, tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.compute_coulomb_energy
+ * (csrc/coulomb/coulomb_interface.cpp:5, csrc/coulomb/coulomb_cuda.cu:17-204).
+ * Gradients dE/dx and dE/dq (dE/dq_i = sum_j k q_j (1/r - [do_shift]/rc), no division by q_i). */
+int tff_coulomb_atom_pairs(int dtype, int64_t natoms, const void *coords, int64_t npairs,
+                           const int64_t *pairs, const void *box, const void *charges,
+                           double coul_constant, double cutoff, int do_shift, void *energy,
+                           void *grad_coords, void *grad_charges, void *workspace,
+                           size_t workspace_bytes, tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.compute_lennard_jones_energy
+ * (csrc/vdw/vdw_interface.cpp:6, csrc/vdw/vdw.cu:83-344).
+ * atom_types == NULL: sigma/epsilon are per pair (P,), gradients per pair.
+ * atom_types != NULL: sigma/epsilon are (ntypes, ntypes) tables, gradients are tables. */
+int tff_lennard_jones_atom_pairs(int dtype, int64_t natoms, const void *coords, int64_t npairs,
+                                 const int64_t *pairs, const void *box, const void *sigma,
+                                 const void *epsilon, double cutoff, const int64_t *atom_types,
+                                 int64_t ntypes, void *energy, void *grad_coords,
+                                 void *grad_sigma, void *grad_epsilon, void *workspace,
+                                 size_t workspace_bytes, tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.compute_multipolar_energy_from_atom_pairs at rank 0
+ * (csrc/multipoles/multipoles_interface.cpp:6, csrc/multipoles/multipoles.cu:24-152,
+ * csrc/multipoles/multipoles_forward.cuh:356-617).
+ * E = prefactor [sum_{pairs, r<=rc} q_i q_j D(r)/r + sum_{excl, r<=rc} q_i q_j (D(r)-1)/r]
+ * with D = erfc(ewald_alpha r) when ewald_alpha >= 0, else D = 1 and no exclusion term.
+ * Gradients dE/dx and dE/dq. */
+int tff_ewald_real_atom_pairs(int dtype, int64_t natoms, const void *coords, const void *box,
+                              int64_t npairs, const int64_t *pairs, int64_t npairs_excl,
+                              const int64_t *pairs_excl, const void *charges, double cutoff,
+                              double ewald_alpha, double prefactor, void *energy,
+                              void *grad_coords, void *grad_charges, void *workspace,
+                              size_t workspace_bytes, tff_stream_t stream);
+
+/* ------------------------------------------------------------------------------
+ * PME reciprocal space (rank 0, order-6 B-splines, cubic K x K x K grid)
+ * --------------------------------------------------------------------------- */
+
+typedef struct tff_pme_plan_s *tff_pme_plan;
+
+/* Creates the cuFFT R2C/C2R plans (cuFFT allocates its own work area here). */
+int tff_pme_plan_create(int dtype, int K, tff_pme_plan *plan);
+int tff_pme_plan_destroy(tff_pme_plan plan);
+size_t tff_pme_workspace_bytes(tff_pme_plan plan, int64_t natoms);
+
+/* Replaces torch.ops.torchff.pme_long_range at rank 0 (csrc/pme/pme_interface.cpp:6-9,
+ * csrc/pme/pme.cu:19-246): forward (spread, rFFT, influence function, irFFT, self term)
+ * AND the gather the reference runs in backward, in one call.
+ * Outputs: energy (scalar) = 1/2 sum q phi - (alpha/sqrt(pi)) sum q^2 in e^2/nm units;
+ * phi (N) = dE/dq (self term included); grad_coords (N,3) = dE/dx. Any output may be NULL
+ * except energy. moduli: the B-spline moduli (K), (K), (K/2+1) as torchff/bsplines.py
+ * computes them (same dtype as coords). */
+int tff_pme_long_range(tff_pme_plan plan, int64_t natoms, const void *coords, const void *box,
+                       const void *charges, double alpha, const void *xmoduli,
+                       const void *ymoduli, const void *zmoduli, void *energy, void *phi,
+                       void *grad_coords, void *workspace, size_t workspace_bytes,
+                       tff_stream_t stream);
+
+/* ------------------------------------------------------------------------------
+ * Fused fixed-charge system: cluster-pair neighbour build + fused real-space
+ * LJ / erfc-Coulomb with exclusion correction + PME, energy and forces in one call.
+ * This is the evaluation of examples/tip3p/model.py:100-133 (nonbonded terms).
+ * --------------------------------------------------------------------------- */
+
+typedef struct tff_system_s *tff_system;
+
+typedef struct tff_system_desc {
+  int dtype;                  /* TFF_F32 (mixed) or TFF_F64 */
+  int64_t natoms;
+  double cutoff;              /* nm */
+  double ewald_alpha;         /* nm^-1 */
+  int pme_grid;               /* K (cubic grid), 0 disables reciprocal space */
+  double coul_constant;       /* 138.935456 kJ mol^-1 nm e^-2 */
+  int max_cluster_neighbors;  /* 0 = default */
+} tff_system_desc;
+
+/* Creates a system, copying per-atom parameters from HOST arrays (float64):
+ * charges (N), sigma (N), epsilon (N) (Lorentz-Berthelot combining) and the exclusion
+ * pairs (nexcl, 2) int64 (both orders implied; self pairs ignored). Excluded pairs get no
+ * LJ and the Ewald exclusion correction -k q_i q_j erf(alpha r)/r. Owns device memory. */
+int tff_system_create(const tff_system_desc *desc, const double *charges, const double *sigma,
+                      const double *epsilon, int64_t nexcl, const int64_t *excl_pairs,
+                      tff_system *sys);
+int tff_system_destroy(tff_system sys);
+/* Overwrites per-atom parameters (device arrays of the system dtype, may be NULL to keep). */
+int tff_system_set_parameters(tff_system sys, const void *charges, const void *sigma,
+                              const void *epsilon, tff_stream_t stream);
+/* Evaluates energy and forces with device-resident inputs. coords (N,3), box (3,3) in the
+ * system dtype; energy (device double, 1) total in kJ/mol; forces (N,3) system dtype,
+ * = -dE/dx; grad_charges (N) optional dE/dq. energy_terms (device double, 4) optional:
+ * real-space pairs, exclusion correction, reciprocal, self. */
+int tff_system_eval(tff_system sys, const void *coords, const void *box, double *energy,
+                    void *forces, void *grad_charges, double *energy_terms, tff_stream_t stream);
+/* Same with HOST buffers: copies coords/box in, evaluates, copies energy/forces out and
+ * synchronises `stream`. coords/box/forces are float64 host arrays whatever the dtype. */
+int tff_system_eval_host(tff_system sys, const double *coords, const double *box,
+                         double *energy, double *forces, tff_stream_t stream);
+/* Device status word of the last evaluation (bit 0: a cluster neighbour list overflowed,
+ * bit 1: fixed-point accumulator overflow guard tripped). Synchronises `stream`. */
+int tff_system_status(tff_system sys, tff_stream_t stream, int *status);
+
+/* Stage timing. A timer holds TFF_TIMER_EVENTS CUDA events; tff_system_eval_timed records
+ * them at the stage boundaries of one evaluation (also inside a CUDA-graph capture, as
+ * event-record nodes): 0 start, 1 cluster build done, 2 real-space tile kernel done,
+ * 3 PME spread + FFTs + influence function done, 4 PME gather done, 5 finalize done.
+ * tff_timer_elapsed_ms waits for event `to` and returns the time between two events. */
+#define TFF_TIMER_EVENTS 6
+typedef struct tff_timer_s *tff_timer;
+int tff_timer_create(tff_timer *timer);
+int tff_timer_destroy(tff_timer timer);
+int tff_timer_elapsed_ms(tff_timer timer, int from, int to, float *ms);
+int tff_system_eval_timed(tff_system sys, const void *coords, const void *box, double *energy,
+                          void *forces, tff_timer timer, tff_stream_t stream);
+/* Number of kernels of this library one tff_system_eval launches (cuFFT's excluded). */
+int tff_system_kernel_launches(tff_system sys);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TFFB200_H */

@@ -1,0 +1,165 @@
+"""Fused system (cluster-pair build + real-space tile kernel + PME) vs the oracle.
+
+FP64: energy 1e-10 relative, forces 1e-8 of their max magnitude. Mixed precision (FP32
+arithmetic, fixed-point forces, FP64 energy): energy 5e-6 relative, force RMS error
+below 1e-5 relative to the FP64 oracle; results bit-identical run to run.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN
+from gpu_util import rel, rel_max, rel_rms, t
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle(wb, coords=None):
+    x = wb.coords if coords is None else coords
+    return O.fixed_charge_energy(x, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
+                                 wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
+                                 138.935456)
+
+
+@pytest.fixture(scope="module")
+def ref216():
+    from torchff_b200.water import water_box_216
+
+    wb = water_box_216()
+    return wb, _oracle(wb)
+
+
+@pytest.fixture(scope="module")
+def ref3000():
+    from torchff_b200.water import water_box_3000
+
+    wb = water_box_3000()
+    return wb, _oracle(wb)
+
+
+def test_oracle_composition_matches_golden(ref216):
+    wb, ref = ref216
+    g = np.load(os.path.join(GOLDEN, "water216.npz"))
+    total = float(g["e_lj"] + g["e_coul"] + 138.935456 * g["e_pme"])
+    assert rel(ref["total"], total) < 1e-12
+
+
+def test_fp64_water216(ref216):
+    from torchff_b200.system import FixedChargeSystem
+
+    wb, ref = ref216
+    sysm = FixedChargeSystem.from_water_box(wb, dtype=torch.float64)
+    out = sysm.evaluate(t(wb.coords), t(wb.box), grad_charges=True, terms=True)
+    assert rel(out["energy"].item(), ref["total"]) < 1e-10
+    assert rel_max(out["forces"], -ref["grad_coords"]) < 1e-8
+    assert rel_max(out["grad_charges"], ref["grad_charges"]) < 1e-8
+    terms = out["terms"].cpu().numpy()
+    assert rel(terms[2] + terms[3], 138.935456 * ref["pme_raw"]) < 1e-10
+    assert sysm.status() == 0
+
+
+def test_mixed_water216(ref216):
+    from torchff_b200.system import FixedChargeSystem
+
+    wb, ref = ref216
+    sysm = FixedChargeSystem.from_water_box(wb, dtype=torch.float32)
+    out = sysm.evaluate(t(wb.coords, torch.float32), t(wb.box, torch.float32))
+    assert rel(out["energy"].item(), ref["total"]) < 5e-6
+    assert rel_rms(out["forces"], -ref["grad_coords"]) < 1e-5
+
+
+def test_mixed_water3000_accuracy_and_determinism(ref3000):
+    from torchff_b200.system import FixedChargeSystem
+
+    wb, ref = ref3000
+    sysm = FixedChargeSystem.from_water_box(wb, dtype=torch.float32)
+    x, b = t(wb.coords, torch.float32), t(wb.box, torch.float32)
+    outs = [sysm.evaluate(x, b) for _ in range(3)]
+    for o in outs[1:]:
+        assert torch.equal(o["energy"], outs[0]["energy"]) and torch.equal(o["forces"], outs[0]["forces"])
+    assert rel(outs[0]["energy"].item(), ref["total"]) < 5e-6
+    assert rel_rms(outs[0]["forces"], -ref["grad_coords"]) < 1e-5
+    assert sysm.status() == 0
+
+
+def test_fp64_water3000(ref3000):
+    from torchff_b200.system import FixedChargeSystem
+
+    wb, ref = ref3000
+    sysm = FixedChargeSystem.from_water_box(wb, dtype=torch.float64)
+    out = sysm.evaluate(t(wb.coords), t(wb.box))
+    assert rel(out["energy"].item(), ref["total"]) < 1e-10
+    assert rel_max(out["forces"], -ref["grad_coords"]) < 1e-8
+
+
+def test_host_entry_point_matches_device(ref216):
+    from torchff_b200.system import FixedChargeSystem
+
+    wb, ref = ref216
+    for dtype in (torch.float32, torch.float64):
+        sysm = FixedChargeSystem.from_water_box(wb, dtype=dtype)
+        dev = sysm.evaluate(t(wb.coords, dtype), t(wb.box, dtype))
+        f = np.zeros_like(wb.coords)
+        e = sysm.evaluate_host(np.ascontiguousarray(wb.coords), np.ascontiguousarray(wb.box), f)
+        assert e == dev["energy"].item()
+        assert np.array_equal(f.astype(np.float32 if dtype == torch.float32 else np.float64),
+                              dev["forces"].cpu().numpy())
+
+
+def test_cuda_graph_replay_matches_eager(ref3000):
+    from torchff_b200.system import FixedChargeSystem
+
+    wb, _ = ref3000
+    sysm = FixedChargeSystem.from_water_box(wb, dtype=torch.float32)
+    x, b = t(wb.coords, torch.float32), t(wb.box, torch.float32)
+    e = torch.empty(1, dtype=torch.float64, device="cuda")
+    f = torch.empty_like(x)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        sysm.evaluate_into(x, b, e, f)
+    torch.cuda.current_stream().wait_stream(s)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        sysm.evaluate_into(x, b, e, f)
+    x.add_(0.001)
+    graph.replay()
+    torch.cuda.synchronize()
+    eager = sysm.evaluate(x, b)
+    assert torch.equal(e, eager["energy"].reshape(1)) and torch.equal(f, eager["forces"])
+
+
+def test_module_autograd_and_charge_gradient(ref216):
+    from torchff_b200.system import FixedChargeNonbonded, FixedChargeSystem
+
+    wb, ref = ref216
+    sysm = FixedChargeSystem.from_water_box(wb, dtype=torch.float64)
+    model = FixedChargeNonbonded(sysm)
+    x = t(wb.coords, grad=True)
+    q = t(wb.charges, grad=True)
+    e = model(x, t(wb.box), q)
+    e.backward()
+    assert rel_max(x.grad, ref["grad_coords"]) < 1e-8
+    assert rel_max(q.grad, ref["grad_charges"]) < 1e-8
+
+
+def test_fused_matches_operator_composition(ref216):
+    """The reference composition through torch.ops.torchff gives the same energy."""
+    from torchff_b200 import PME, MultipolarInteraction, NeighborList, Vdw
+
+    wb, ref = ref216
+    x, b, q = t(wb.coords, grad=True), t(wb.box), t(wb.charges)
+    nbl = NeighborList(wb.natoms, exclusions=torch.tensor(wb.nblist_exclusions), algorithm="cell_list").cuda()
+    pairs, _ = nbl(x.detach(), b, wb.cutoff, 200000, padding=True)
+    e_lj = Vdw("LennardJones", use_customized_ops=True, use_type_pairs=True)(
+        x, pairs, b, t(wb.sigma_table), t(wb.epsilon_table), wb.cutoff, atom_types=t(wb.atom_types, torch.int64))
+    e_c = MultipolarInteraction(0, wb.cutoff, wb.alpha, 138.935456)(x, b, pairs, q,
+                                                                     pairs_excl=t(wb.coulomb_exclusions, torch.int64))
+    e_p = PME(wb.alpha, wb.grid, 0, use_customized_ops=True).cuda()(x, b, q) * 138.935456
+    e = e_lj + e_c + e_p
+    e.backward()
+    assert rel(e.item(), ref["total"]) < 1e-10
+    assert rel_max(x.grad, ref["grad_coords"]) < 1e-8

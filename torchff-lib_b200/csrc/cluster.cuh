@@ -1,0 +1,384 @@
+// Cluster build shared by the cell-list neighbour list and the fused real-space kernel.
+//
+// 1. cell_keys:      fractional coordinates wrapped to [0,1), cell on an nc^3 grid
+//                    (about 4 atoms per cell), Morton key, per-key histogram.
+// 2. scan_keys:      exclusive scan of the histogram (one block).
+// 3. scatter_atoms:  atoms into key buckets (slot order inside a bucket is arbitrary).
+// 4. sort_buckets:   each bucket sorted by atom index -> deterministic order; writes the
+//                    sorted SoA (wrapped position + charge as a 4-vector, original index,
+//                    inverse map, fractional position) and pads to a multiple of 32.
+// 5. cluster_bounds: one warp per 32-atom cluster: fractional bounding box.
+// 6. cluster_neighbors: one warp per cluster scans all clusters in index order and keeps
+//                    those whose boxes can hold a pair within the cutoff (order of the
+//                    list is deterministic). `half` keeps only J <= I.
+//
+// The Morton order of ~4-atom cells makes 32 consecutive atoms a compact blob (about a
+// 2x2x2 block of cells), which is what the 32x32 warp tiles need.
+#pragma once
+
+#include "tff_common.cuh"
+
+namespace tff {
+
+template <class T> struct V4;
+template <> struct V4<float> { using type = float4; };
+struct __align__(16) D4 { double x, y, z, w; };
+template <> struct V4<double> { using type = D4; };
+
+__device__ __forceinline__ D4 make_v4(double x, double y, double z, double w) { return D4{x, y, z, w}; }
+__device__ __forceinline__ float4 make_v4(float x, float y, float z, float w) { return make_float4(x, y, z, w); }
+
+struct ClusterLayout {
+  int nc = 1, bits = 0;
+  int64_t nkeys = 1, natoms = 0, nclusters = 0, npad = 0;
+  int cap = 0;
+  size_t keys, hist, fill, status, tmp, sidx, inv, pos, frac, bc, bh, nbr, ncount, boxinfo;
+  size_t zero_off, zero_bytes, bytes;
+};
+
+inline unsigned morton_spread_host(unsigned v) {
+  v &= 0x3ff;
+  v = (v | (v << 16)) & 0x030000FF;
+  v = (v | (v << 8)) & 0x0300F00F;
+  v = (v | (v << 4)) & 0x030C30C3;
+  v = (v | (v << 2)) & 0x09249249;
+  return v;
+}
+
+inline ClusterLayout cluster_layout(int dtype, int64_t natoms, int cap) {
+  ClusterLayout L;
+  L.natoms = natoms;
+  int nc = (int)floor(cbrt((double)natoms / 4.0));
+  nc = std::max(1, std::min(nc, 128));
+  int bits = 0;
+  while ((1 << bits) < nc) ++bits;
+  L.nc = nc;
+  L.bits = bits;
+  L.nkeys = (int64_t)1 << (3 * bits);
+  L.nclusters = (natoms + kWarp - 1) / kWarp;
+  L.npad = L.nclusters * kWarp;
+  L.cap = cap;
+  const size_t tsz = dtype == TFF_F64 ? 8 : 4;
+  Carver c(nullptr);
+  // zero-initialised region first: hist, fill, status
+  L.hist = c.off; c.take<unsigned>(L.nkeys + 1);
+  L.fill = (c.off + 255) & ~size_t(255); c.take<unsigned>(L.nkeys);
+  L.status = (c.off + 255) & ~size_t(255); c.take<unsigned>(64);
+  L.zero_off = 0;
+  L.zero_bytes = c.bytes();
+  L.keys = (c.off + 255) & ~size_t(255); c.take<unsigned>(natoms);
+  L.tmp = (c.off + 255) & ~size_t(255); c.take<int>(natoms);
+  L.sidx = (c.off + 255) & ~size_t(255); c.take<int>(L.npad);
+  L.inv = (c.off + 255) & ~size_t(255); c.take<int>(natoms);
+  L.pos = (c.off + 255) & ~size_t(255); c.take<char>(L.npad * 4 * tsz);
+  L.frac = (c.off + 255) & ~size_t(255); c.take<char>(L.npad * 4 * tsz);
+  L.bc = (c.off + 255) & ~size_t(255); c.take<char>(L.nclusters * 4 * tsz);
+  L.bh = (c.off + 255) & ~size_t(255); c.take<char>(L.nclusters * 4 * tsz);
+  L.nbr = (c.off + 255) & ~size_t(255); c.take<int>((size_t)L.nclusters * cap);
+  L.ncount = (c.off + 255) & ~size_t(255); c.take<int>(L.nclusters);
+  L.boxinfo = (c.off + 255) & ~size_t(255); c.take<double>(32);
+  L.bytes = c.bytes();
+  return L;
+}
+
+// Pointers into one workspace.
+template <class T>
+struct ClusterData {
+  using V = typename V4<T>::type;
+  unsigned *keys, *hist, *fill, *status;
+  int *tmp, *sidx, *inv, *nbr, *ncount;
+  V *pos, *frac, *bc, *bh;
+  double *boxinfo;  // [0..8] box, [9..17] inv, [18] ortho flag, [19..21] perpendicular widths
+  int nc, bits, cap;
+  int64_t natoms, nclusters, npad;
+};
+
+template <class T>
+inline ClusterData<T> cluster_data(const ClusterLayout &L, void *ws) {
+  char *b = static_cast<char *>(ws);
+  ClusterData<T> d;
+  using V = typename ClusterData<T>::V;
+  d.keys = reinterpret_cast<unsigned *>(b + L.keys);
+  d.hist = reinterpret_cast<unsigned *>(b + L.hist);
+  d.fill = reinterpret_cast<unsigned *>(b + L.fill);
+  d.status = reinterpret_cast<unsigned *>(b + L.status);
+  d.tmp = reinterpret_cast<int *>(b + L.tmp);
+  d.sidx = reinterpret_cast<int *>(b + L.sidx);
+  d.inv = reinterpret_cast<int *>(b + L.inv);
+  d.nbr = reinterpret_cast<int *>(b + L.nbr);
+  d.ncount = reinterpret_cast<int *>(b + L.ncount);
+  d.pos = reinterpret_cast<V *>(b + L.pos);
+  d.frac = reinterpret_cast<V *>(b + L.frac);
+  d.bc = reinterpret_cast<V *>(b + L.bc);
+  d.bh = reinterpret_cast<V *>(b + L.bh);
+  d.boxinfo = reinterpret_cast<double *>(b + L.boxinfo);
+  d.nc = L.nc;
+  d.bits = L.bits;
+  d.cap = L.cap;
+  d.natoms = L.natoms;
+  d.nclusters = L.nclusters;
+  d.npad = L.npad;
+  return d;
+}
+
+__device__ __forceinline__ unsigned morton_spread(unsigned v) {
+  v &= 0x3ff;
+  v = (v | (v << 16)) & 0x030000FF;
+  v = (v | (v << 8)) & 0x0300F00F;
+  v = (v | (v << 4)) & 0x030C30C3;
+  v = (v | (v << 2)) & 0x09249249;
+  return v;
+}
+
+// Box facts used by the cluster search: inverse, orthorhombic flag, perpendicular widths.
+template <class T>
+__global__ void box_info_kernel(const T *box, double *info) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Box b;
+  load_box(box, b);
+  for (int k = 0; k < 9; ++k) {
+    info[k] = b.m[k];
+    info[9 + k] = b.inv[k];
+  }
+  const double *m = b.m;
+  bool ortho = m[1] == 0.0 && m[2] == 0.0 && m[3] == 0.0 && m[5] == 0.0 && m[6] == 0.0 && m[7] == 0.0;
+  info[18] = ortho ? 1.0 : 0.0;
+  // width along lattice direction d = V / |cross of the other two rows|
+  for (int d = 0; d < 3; ++d) {
+    const double *u = m + 3 * ((d + 1) % 3);
+    const double *v = m + 3 * ((d + 2) % 3);
+    double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2], cz = u[0] * v[1] - u[1] * v[0];
+    info[19 + d] = b.vol / sqrt(cx * cx + cy * cy + cz * cz);
+  }
+}
+
+template <class T>
+__global__ void cell_keys_kernel(const T *x, int64_t n, ClusterData<T> d) {
+  const double *inv = d.boxinfo + 9;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double rx = x[3 * i], ry = x[3 * i + 1], rz = x[3 * i + 2];
+    double f[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double v = rx * inv[c] + ry * inv[3 + c] + rz * inv[6 + c];
+      v -= floor(v);
+      if (v >= 1.0) v = 0.0;  // guards rounding of tiny negatives
+      f[c] = v;
+    }
+    unsigned cell[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) cell[c] = min((unsigned)(f[c] * d.nc), (unsigned)(d.nc - 1));
+    unsigned key = (morton_spread(cell[0]) << 2) | (morton_spread(cell[1]) << 1) | morton_spread(cell[2]);
+    d.keys[i] = key;
+    atomicAdd(&d.hist[key], 1u);
+  }
+}
+
+// Exclusive scan of hist[0..nkeys) in place; hist[nkeys] = total. One block of 1024.
+static __global__ void scan_keys_kernel(unsigned *hist, int64_t nkeys) {
+  __shared__ unsigned s_warp[32];
+  __shared__ unsigned s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int64_t base = 0; base < nkeys; base += blockDim.x) {
+    int64_t k = base + threadIdx.x;
+    unsigned v = (k < nkeys) ? hist[k] : 0u;
+    unsigned incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      unsigned t = (lane < (int)(blockDim.x >> 5)) ? s_warp[lane] : 0u;
+      unsigned ti = t;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        unsigned y = __shfl_up_sync(kFull, ti, o);
+        if (lane >= o) ti += y;
+      }
+      s_warp[lane] = ti - t;  // exclusive warp offsets
+    }
+    __syncthreads();
+    unsigned carry = s_carry;
+    if (k < nkeys) hist[k] = carry + s_warp[w] + incl - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) s_carry = carry + s_warp[w] + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) hist[nkeys] = s_carry;
+}
+
+template <class T>
+__global__ void scatter_atoms_kernel(int64_t n, ClusterData<T> d) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    unsigned key = d.keys[i];
+    unsigned slot = d.hist[key] + atomicAdd(&d.fill[key], 1u);
+    d.tmp[slot] = (int)i;
+  }
+}
+
+// One thread per key: insertion-sort the bucket by atom index, then write the sorted SoA.
+// q may be NULL (charge slot = 0).
+template <class T>
+__global__ void sort_buckets_kernel(const T *x, const T *q, int64_t nkeys, ClusterData<T> d) {
+  const double *m = d.boxinfo;
+  const double *inv = d.boxinfo + 9;
+  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nkeys; k += gstride) {
+    const unsigned b0 = d.hist[k], b1 = d.hist[k + 1];
+    for (unsigned a = b0 + 1; a < b1; ++a) {
+      int v = d.tmp[a];
+      unsigned c = a;
+      while (c > b0 && d.tmp[c - 1] > v) {
+        d.tmp[c] = d.tmp[c - 1];
+        --c;
+      }
+      d.tmp[c] = v;
+    }
+    for (unsigned s = b0; s < b1; ++s) {
+      const int i = d.tmp[s];
+      double rx = x[3 * i], ry = x[3 * i + 1], rz = x[3 * i + 2];
+      double f[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double v = rx * inv[c] + ry * inv[3 + c] + rz * inv[6 + c];
+        v -= floor(v);
+        if (v >= 1.0) v = 0.0;
+        f[c] = v;
+      }
+      double wx = f[0] * m[0] + f[1] * m[3] + f[2] * m[6];
+      double wy = f[0] * m[1] + f[1] * m[4] + f[2] * m[7];
+      double wz = f[0] * m[2] + f[1] * m[5] + f[2] * m[8];
+      d.pos[s] = make_v4((T)wx, (T)wy, (T)wz, q ? q[i] : T(0));
+      d.frac[s] = make_v4((T)f[0], (T)f[1], (T)f[2], T(0));
+      d.sidx[s] = i;
+      d.inv[i] = (int)s;
+    }
+  }
+  // padding slots
+  for (int64_t s = d.natoms + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < d.npad; s += gstride) {
+    d.sidx[s] = -1;
+    d.pos[s] = make_v4(T(0), T(0), T(0), T(0));
+    d.frac[s] = make_v4(T(0), T(0), T(0), T(0));
+  }
+}
+
+// One warp per cluster: bounding box in fractional coordinates. The box is taken around
+// the first atom's image so that a cluster straddling the periodic boundary stays compact.
+template <class T>
+__global__ void cluster_bounds_kernel(ClusterData<T> d) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < d.nclusters; c += nw) {
+    const int64_t s = c * kWarp + lane;
+    const bool valid = d.sidx[s] >= 0;
+    auto f = d.frac[s];
+    T fx = f.x, fy = f.y, fz = f.z;
+    const T ax = __shfl_sync(kFull, fx, 0), ay = __shfl_sync(kFull, fy, 0), az = __shfl_sync(kFull, fz, 0);
+    fx -= ax; fy -= ay; fz -= az;
+    fx -= floor(fx + T(0.5)); fy -= floor(fy + T(0.5)); fz -= floor(fz + T(0.5));
+    T lo[3] = {valid ? fx : T(1e30), valid ? fy : T(1e30), valid ? fz : T(1e30)};
+    T hi[3] = {valid ? fx : T(-1e30), valid ? fy : T(-1e30), valid ? fz : T(-1e30)};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = min(lo[k], __shfl_xor_sync(kFull, lo[k], o));
+        hi[k] = max(hi[k], __shfl_xor_sync(kFull, hi[k], o));
+      }
+    }
+    if (lane == 0) {
+      d.bc[c] = make_v4(ax + T(0.5) * (lo[0] + hi[0]), ay + T(0.5) * (lo[1] + hi[1]),
+                        az + T(0.5) * (lo[2] + hi[2]), T(0));
+      d.bh[c] = make_v4(T(0.5) * (hi[0] - lo[0]), T(0.5) * (hi[1] - lo[1]), T(0.5) * (hi[2] - lo[2]), T(0));
+    }
+  }
+}
+
+// Whether clusters I and J can hold a pair within rc. Fractional per-dimension gaps use
+// the nearest periodic image of the centres (per dimension, the minimum over all images);
+// orthorhombic boxes test sum_d (gap_d L_d)^2 <= rc^2 (exact for boxes), other boxes the
+// conservative max_d gap_d w_d <= rc with w_d the perpendicular widths.
+template <class T>
+__device__ __forceinline__ bool clusters_may_interact(const typename V4<T>::type &ci, const typename V4<T>::type &hi,
+                                                      const typename V4<T>::type &cj, const typename V4<T>::type &hj,
+                                                      const double *info, double rc) {
+  double g[3];
+  double dc[3] = {(double)ci.x - (double)cj.x, (double)ci.y - (double)cj.y, (double)ci.z - (double)cj.z};
+  double hs[3] = {(double)hi.x + (double)hj.x, (double)hi.y + (double)hj.y, (double)hi.z + (double)hj.z};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double v = dc[k] - floor(dc[k] + 0.5);
+    // 1e-6 margin in fractional units absorbs the FP32 rounding of centres and extents
+    g[k] = fmax(0.0, fabs(v) - hs[k] - 1e-6);
+  }
+  if (info[18] != 0.0) {
+    double x = g[0] * info[0], y = g[1] * info[4], z = g[2] * info[8];
+    return x * x + y * y + z * z <= rc * rc;
+  }
+  double m = fmax(g[0] * info[19], fmax(g[1] * info[20], g[2] * info[21]));
+  return m <= rc;
+}
+
+template <class T>
+__global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t I = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); I < d.nclusters; I += nw) {
+    const auto ci = d.bc[I];
+    const auto hi = d.bh[I];
+    int count = 0;
+    const int64_t jend = half ? (I + 1) : d.nclusters;
+    for (int64_t base = 0; base < jend; base += kWarp) {
+      const int64_t J = base + lane;
+      bool ok = false;
+      if (J < jend) ok = clusters_may_interact<T>(ci, hi, d.bc[J], d.bh[J], d.boxinfo, rc);
+      const unsigned m = __ballot_sync(kFull, ok);
+      if (ok) {
+        const int r = count + __popc(m & ((1u << lane) - 1u));
+        if (r < d.cap) d.nbr[I * d.cap + r] = (int)J;
+      }
+      count += __popc(m);
+    }
+    if (lane == 0) {
+      d.ncount[I] = min(count, d.cap);
+      if (count > d.cap) atomicOr(&d.status[0], 1u);
+    }
+  }
+}
+
+// Host driver for steps 1-6 on `stream`.
+template <class T>
+int build_clusters(const ClusterLayout &L, const ClusterData<T> &d, void *ws, const T *x, const T *q,
+                   const T *box, double rc, int half, cudaStream_t s) {
+  char *b = static_cast<char *>(ws);
+  TFF_CUDA(cudaMemsetAsync(b + L.zero_off, 0, L.zero_bytes, s));
+  box_info_kernel<T><<<1, 32, 0, s>>>(box, d.boxinfo);
+  TFF_LAUNCHED();
+  if (L.natoms == 0) return TFF_OK;
+  const int sms = sm_count();
+  const int nb_atoms = (int)std::max<int64_t>(1, std::min<int64_t>((L.natoms + 255) / 256, sms * 8));
+  cell_keys_kernel<T><<<nb_atoms, 256, 0, s>>>(x, L.natoms, d);
+  TFF_LAUNCHED();
+  scan_keys_kernel<<<1, 1024, 0, s>>>(d.hist, L.nkeys);
+  TFF_LAUNCHED();
+  scatter_atoms_kernel<T><<<nb_atoms, 256, 0, s>>>(L.natoms, d);
+  TFF_LAUNCHED();
+  const int nb_keys = (int)std::max<int64_t>(1, std::min<int64_t>((std::max(L.nkeys, L.npad - L.natoms) + 127) / 128, sms * 16));
+  sort_buckets_kernel<T><<<nb_keys, 128, 0, s>>>(x, q, L.nkeys, d);
+  TFF_LAUNCHED();
+  const int nb_cl = (int)std::max<int64_t>(1, std::min<int64_t>((L.nclusters + 3) / 4, sms * 16));
+  cluster_bounds_kernel<T><<<nb_cl, 128, 0, s>>>(d);
+  TFF_LAUNCHED();
+  cluster_neighbors_kernel<T><<<nb_cl, 128, 0, s>>>(d, rc, half);
+  TFF_LAUNCHED();
+  return TFF_OK;
+}
+
+}  // namespace tff

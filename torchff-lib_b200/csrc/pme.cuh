@@ -1,0 +1,379 @@
+// Rank-0 smooth PME (order-6 B-splines) on a cubic K^3 grid.
+//
+//   spread   : Q(g) = sum_i q_i M6(u_i,x) M6(u_i,y) M6(u_i,z)   (fixed-point or FP64 atomics)
+//   [to_real]: fixed-point grid -> FP32 (mixed precision)
+//   R2C FFT  : S(k)                                             (cuFFT)
+//   convolve : S(k) *= C(k)/theta(k)^2, E_rec = 1/2 sum_k C |S|^2/theta^2 (FP64, fixed order)
+//   C2R FFT  : Phi(g)                                           (cuFFT, unnormalised)
+//   gather   : phi_i = sum_g theta_i(g) Phi(g), dE/dx_i = q_i grad phi_i,
+//              dE/dq_i = phi_i - 2 a q_i / sqrt(pi), E_self = -(a/sqrt(pi)) sum q^2
+//
+// Conventions follow the reference (torchff/pme_ref.py:11-469, csrc/pme/kernels.cuh):
+// u = K * (box^-T r) per lattice direction, m0 = ceil(u), the 6 stencil points are
+// m0-3 .. m0+2 with weights M6((m0 - u) + k), grid index gx*K^2 + gy*K + gz, and
+// the signed frequency of FFT index i is i for 2i < K, else i - K.
+#pragma once
+
+#include <cufft.h>
+
+#include "cluster.cuh"
+
+namespace tff {
+
+constexpr int kPmeBlock = 256;
+
+// Per-atom stencil: origin index (already wrapped into [0,K)) and the 3x6 weights.
+template <class T>
+struct Stencil {
+  int g0[3];
+  T val[3][6];
+  T der[3][6];
+};
+
+// recip[d*3 + c] = K * inv[c][d]: u_d = sum_c recip[d][c] r_c
+template <class T>
+__device__ __forceinline__ void make_stencil(double rx, double ry, double rz, const double *recip, int K,
+                                             Stencil<T> &s) {
+  const double r[3] = {rx, ry, rz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double u = recip[3 * d] * r[0] + recip[3 * d + 1] * r[1] + recip[3 * d + 2] * r[2];
+    const double m0 = ceil(u);
+    const T w = (T)(m0 - u);
+    bspline6<T>(w, s.val[d], s.der[d]);
+    long long g = (long long)m0 - 3;
+    g %= K;
+    if (g < 0) g += K;
+    s.g0[d] = (int)g;
+  }
+}
+
+struct PmeShared {
+  double recip[9];
+  double inv[9];
+  double vol;
+};
+
+template <class T>
+__device__ __forceinline__ void load_pme_shared(const T *box, int K, PmeShared &sh) {
+  Box b;
+  load_box(box, b);
+  for (int d = 0; d < 3; ++d)
+    for (int c = 0; c < 3; ++c) sh.recip[3 * d + c] = (double)K * b.inv[3 * c + d];
+  for (int k = 0; k < 9; ++k) sh.inv[k] = b.inv[k];
+  sh.vol = b.vol;
+}
+
+// Atom sources: plain (caller arrays) or cluster-sorted (wrapped positions, charge in .w).
+template <class T>
+struct PlainAtoms {
+  const T *x;
+  const T *q;
+  int64_t n;
+  __device__ __forceinline__ bool get(int64_t t, double &rx, double &ry, double &rz, T &qi) const {
+    if (t >= n) return false;
+    rx = x[3 * t]; ry = x[3 * t + 1]; rz = x[3 * t + 2];
+    qi = q[t];
+    return true;
+  }
+};
+
+template <class T>
+struct SortedAtoms {
+  const typename V4<T>::type *pos;
+  const int *sidx;
+  int64_t npad;
+  __device__ __forceinline__ bool get(int64_t t, double &rx, double &ry, double &rz, T &qi) const {
+    if (t >= npad || sidx[t] < 0) return false;
+    const auto p = pos[t];
+    rx = p.x; ry = p.y; rz = p.z;
+    qi = p.w;
+    return true;
+  }
+};
+
+template <class T, class Atoms>
+__global__ void __launch_bounds__(kPmeBlock) pme_spread_kernel(Atoms atoms, int64_t nthreads, const T *box, int K,
+                                                               typename Acc<T>::S *grid) {
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
+  __syncthreads();
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nthreads; t += stride) {
+    double rx, ry, rz;
+    T q;
+    if (!atoms.get(t, rx, ry, rz, q)) continue;
+    Stencil<T> s;
+    make_stencil<T>(rx, ry, rz, sh.recip, K, s);
+    int gx = s.g0[0];
+#pragma unroll 1
+    for (int a = 0; a < 6; ++a) {
+      const T wx = q * s.val[0][a];
+      int gy = s.g0[1];
+#pragma unroll
+      for (int b = 0; b < 6; ++b) {
+        const T wxy = wx * s.val[1][b];
+        const int64_t row = ((int64_t)gx * K + gy) * K;
+        int gz = s.g0[2];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          Acc<T>::add(&grid[row + gz], (double)(wxy * s.val[2][c]));
+          gz = (gz + 1 == K) ? 0 : gz + 1;
+        }
+        gy = (gy + 1 == K) ? 0 : gy + 1;
+      }
+      gx = (gx + 1 == K) ? 0 : gx + 1;
+    }
+  }
+}
+
+static __global__ void pme_fix_to_real_kernel(const unsigned long long *gi, float *gf, int64_t n) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    gf[k] = (float)from_fix(gi[k]);
+}
+
+template <class T> struct CplxOf;
+template <> struct CplxOf<float> { using type = cufftComplex; };
+template <> struct CplxOf<double> { using type = cufftDoubleComplex; };
+
+template <class T>
+__global__ void __launch_bounds__(kPmeBlock) pme_convolve_kernel(typename CplxOf<T>::type *S, const T *box, int K,
+                                                                 double alpha, const T *xmod, const T *ymod,
+                                                                 const T *zmod, double *partials, unsigned *ticket,
+                                                                 double *e_rec) {
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
+  __syncthreads();
+  const int Kz = K / 2 + 1;
+  const int64_t total = (int64_t)K * K * Kz;
+  const double four_pi_over_v = 4.0 * 3.14159265358979323846 / sh.vol;
+  const double two_pi = 2.0 * 3.14159265358979323846;
+  const double inv4a2 = 1.0 / (4.0 * alpha * alpha);
+  double e = 0.0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int iz = (int)(t % Kz);
+    const int iy = (int)((t / Kz) % K);
+    const int ix = (int)(t / ((int64_t)Kz * K));
+    const double mx = (2 * ix < K) ? ix : ix - K;
+    const double my = (2 * iy < K) ? iy : iy - K;
+    const double mz = (2 * iz < K) ? iz : iz - K;
+    double factor = 0.0;
+    if (t != 0) {
+      // k_c = 2 pi sum_d m_d inv[c][d]
+      const double kx = two_pi * (mx * sh.inv[0] + my * sh.inv[1] + mz * sh.inv[2]);
+      const double ky = two_pi * (mx * sh.inv[3] + my * sh.inv[4] + mz * sh.inv[5]);
+      const double kz = two_pi * (mx * sh.inv[6] + my * sh.inv[7] + mz * sh.inv[8]);
+      const double ksq = kx * kx + ky * ky + kz * kz;
+      const double th = (double)xmod[ix] * (double)ymod[iy] * (double)zmod[iz];
+      factor = four_pi_over_v * exp(-ksq * inv4a2) / (ksq * th * th);
+    }
+    auto v = S[t];
+    const double re = v.x, im = v.y;
+    const double w = (iz == 0 || 2 * iz == K) ? 1.0 : 2.0;
+    e += w * factor * (re * re + im * im);
+    v.x = (T)(re * factor);
+    v.y = (T)(im * factor);
+    S[t] = v;
+  }
+  grid_sum<kPmeBlock>(0.5 * e, partials, ticket, e_rec, false);
+}
+
+// Gather outputs: plain caller arrays (original order) ...
+template <class T>
+struct PlainGatherOut {
+  T *phi;    // dE/dq (N), nullable
+  T *grad;   // dE/dx (N,3), nullable
+  __device__ __forceinline__ void put(int64_t t, double phi_t, double gx, double gy, double gz) const {
+    if (phi) phi[t] = (T)phi_t;
+    if (grad) {
+      grad[3 * t] = (T)gx;
+      grad[3 * t + 1] = (T)gy;
+      grad[3 * t + 2] = (T)gz;
+    }
+  }
+};
+
+// ... or cluster-sorted accumulators of the fused system (scaled by the Coulomb constant).
+template <class T>
+struct SortedGatherOut {
+  typename Acc<T>::S *gx;  // (npad, 3) sorted slots, dE/dx
+  typename Acc<T>::S *gq;  // (npad) sorted slots, dE/dq
+  double scale;
+  __device__ __forceinline__ void put(int64_t t, double phi_t, double x, double y, double z) const {
+    Acc<T>::add(&gx[3 * t], scale * x);
+    Acc<T>::add(&gx[3 * t + 1], scale * y);
+    Acc<T>::add(&gx[3 * t + 2], scale * z);
+    if (gq) Acc<T>::add(&gq[t], scale * phi_t);
+  }
+};
+
+template <class T, class Atoms, class Out>
+__global__ void __launch_bounds__(kPmeBlock) pme_gather_kernel(Atoms atoms, int64_t nthreads, const T *box, int K,
+                                                               const T *Phi, double alpha, Out out, double *partials,
+                                                               unsigned *ticket, double *e_self, const double *e_rec,
+                                                               double e_scale, T *energy_out) {
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
+  __syncthreads();
+  const double a_rpi = alpha / 1.7724538509055160273;
+  double e = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nthreads; t += stride) {
+    double rx, ry, rz;
+    T q;
+    if (!atoms.get(t, rx, ry, rz, q)) continue;
+    Stencil<T> s;
+    make_stencil<T>(rx, ry, rz, sh.recip, K, s);
+    double phi = 0.0, du0 = 0.0, du1 = 0.0, du2 = 0.0;
+    int gx = s.g0[0];
+#pragma unroll 1
+    for (int a = 0; a < 6; ++a) {
+      int gy = s.g0[1];
+      double p_a = 0.0, d1_a = 0.0, d2_a = 0.0;
+#pragma unroll
+      for (int b = 0; b < 6; ++b) {
+        const int64_t row = ((int64_t)gx * K + gy) * K;
+        int gz = s.g0[2];
+        T pz = T(0), dz = T(0);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          const T g = Phi[row + gz];
+          pz += g * s.val[2][c];
+          dz += g * s.der[2][c];
+          gz = (gz + 1 == K) ? 0 : gz + 1;
+        }
+        p_a += (double)(pz * s.val[1][b]);
+        d1_a += (double)(pz * s.der[1][b]);
+        d2_a += (double)(dz * s.val[1][b]);
+        gy = (gy + 1 == K) ? 0 : gy + 1;
+      }
+      phi += p_a * (double)s.val[0][a];
+      du0 += p_a * (double)s.der[0][a];
+      du1 += d1_a * (double)s.val[0][a];
+      du2 += d2_a * (double)s.val[0][a];
+      gx = (gx + 1 == K) ? 0 : gx + 1;
+    }
+    // u_d = m0 - frac_d + const, so d(stencil u)/dr_c = -recip[d][c]
+    const double qd = (double)q;
+    const double gxv = -qd * (du0 * sh.recip[0] + du1 * sh.recip[3] + du2 * sh.recip[6]);
+    const double gyv = -qd * (du0 * sh.recip[1] + du1 * sh.recip[4] + du2 * sh.recip[7]);
+    const double gzv = -qd * (du0 * sh.recip[2] + du1 * sh.recip[5] + du2 * sh.recip[8]);
+    out.put(t, phi - 2.0 * a_rpi * qd, gxv, gyv, gzv);
+    e -= a_rpi * qd * qd;
+  }
+  const bool last = grid_sum<kPmeBlock>(e, partials, ticket, e_self, false);
+  if (last && threadIdx.x == 0 && energy_out) energy_out[0] = (T)(e_scale * (*e_rec + *e_self));
+}
+
+// Scratch layout of one PME evaluation.
+struct PmeLayout {
+  int K;
+  int64_t ngrid, ncplx;
+  size_t fix, real, cplx, partials, tickets, energies, bytes;
+  size_t zero_off, zero_bytes;
+};
+
+inline PmeLayout pme_layout(int dtype, int K) {
+  PmeLayout L{};
+  L.K = K;
+  L.ngrid = (int64_t)K * K * K;
+  L.ncplx = (int64_t)K * K * (K / 2 + 1);
+  const size_t ts = dtype == TFF_F64 ? 8 : 4;
+  Carver c(nullptr);
+  // zeroed on every evaluation: reduction tickets, energies, the accumulation grid
+  L.tickets = c.off; c.take<unsigned>(64);
+  L.energies = (c.off + 255) & ~size_t(255); c.take<double>(8);
+  L.fix = (c.off + 255) & ~size_t(255); c.take<char>(L.ngrid * 8);  // u64 fixed point (mixed) / double (FP64)
+  L.zero_off = 0;
+  L.zero_bytes = c.bytes();
+  L.real = (c.off + 255) & ~size_t(255); c.take<char>(dtype == TFF_F64 ? 0 : L.ngrid * ts);
+  L.cplx = (c.off + 255) & ~size_t(255); c.take<char>(L.ncplx * 2 * ts);
+  L.partials = (c.off + 255) & ~size_t(255); c.take<double>(8192);
+  L.bytes = c.bytes();
+  return L;
+}
+
+struct PmePlanImpl {
+  int dtype;
+  int K;
+  int device;
+  cufftHandle r2c, c2r;
+};
+
+int pme_cufft_fail(cufftResult r, const char *what);
+
+}  // namespace tff
+
+struct tff_pme_plan_s {
+  tff::PmePlanImpl impl;
+};
+
+namespace tff {
+
+// Enqueue spread -> FFT -> convolve -> FFT on `s`; leaves the potential grid Phi in
+// (T*)(ws + L.real) (mixed) or (T*)(ws + L.fix) (FP64) and returns it through *phi_grid.
+template <class T, class Atoms>
+int pme_grid_phase(const PmePlanImpl &p, const PmeLayout &L, char *ws, Atoms atoms, int64_t nthreads, const T *box,
+                   double alpha, const T *xmod, const T *ymod, const T *zmod, cudaStream_t s, T **phi_grid) {
+  using S = typename Acc<T>::S;
+  const int K = p.K;
+  TFF_CUDA(cudaMemsetAsync(ws + L.zero_off, 0, L.zero_bytes, s));
+  const int sms = sm_count();
+  S *grid = reinterpret_cast<S *>(ws + L.fix);
+  if (nthreads > 0) {
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((nthreads + kPmeBlock - 1) / kPmeBlock, sms * 8));
+    pme_spread_kernel<T, Atoms><<<nb, kPmeBlock, 0, s>>>(atoms, nthreads, box, K, grid);
+    TFF_LAUNCHED();
+  }
+  T *real;
+  if (sizeof(T) == 4) {
+    real = reinterpret_cast<T *>(ws + L.real);
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((L.ngrid + 255) / 256, sms * 8));
+    pme_fix_to_real_kernel<<<nb, 256, 0, s>>>(reinterpret_cast<unsigned long long *>(grid),
+                                              reinterpret_cast<float *>(real), L.ngrid);
+    TFF_LAUNCHED();
+  } else {
+    real = reinterpret_cast<T *>(grid);
+  }
+  auto *cplx = reinterpret_cast<typename CplxOf<T>::type *>(ws + L.cplx);
+  cufftResult r;
+  if ((r = cufftSetStream(p.r2c, s)) != CUFFT_SUCCESS) return pme_cufft_fail(r, "cufftSetStream");
+  if ((r = cufftSetStream(p.c2r, s)) != CUFFT_SUCCESS) return pme_cufft_fail(r, "cufftSetStream");
+  if (sizeof(T) == 4)
+    r = cufftExecR2C(p.r2c, reinterpret_cast<cufftReal *>(real), reinterpret_cast<cufftComplex *>(cplx));
+  else
+    r = cufftExecD2Z(p.r2c, reinterpret_cast<cufftDoubleReal *>(real), reinterpret_cast<cufftDoubleComplex *>(cplx));
+  if (r != CUFFT_SUCCESS) return pme_cufft_fail(r, "forward FFT");
+  double *partials = reinterpret_cast<double *>(ws + L.partials);
+  unsigned *tickets = reinterpret_cast<unsigned *>(ws + L.tickets);
+  double *energies = reinterpret_cast<double *>(ws + L.energies);
+  {
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((L.ncplx + kPmeBlock - 1) / kPmeBlock, sms * 4));
+    pme_convolve_kernel<T><<<nb, kPmeBlock, 0, s>>>(cplx, box, K, alpha, xmod, ymod, zmod, partials, tickets,
+                                                    energies);
+    TFF_LAUNCHED();
+  }
+  if (sizeof(T) == 4)
+    r = cufftExecC2R(p.c2r, reinterpret_cast<cufftComplex *>(cplx), reinterpret_cast<cufftReal *>(real));
+  else
+    r = cufftExecZ2D(p.c2r, reinterpret_cast<cufftDoubleComplex *>(cplx), reinterpret_cast<cufftDoubleReal *>(real));
+  if (r != CUFFT_SUCCESS) return pme_cufft_fail(r, "inverse FFT");
+  *phi_grid = real;
+  return TFF_OK;
+}
+
+template <class T, class Atoms, class Out>
+int pme_gather_phase(const PmePlanImpl &p, const PmeLayout &L, char *ws, Atoms atoms, int64_t nthreads, const T *box,
+                     double alpha, const T *phi_grid, Out out, double e_scale, T *energy_out, cudaStream_t s) {
+  double *partials = reinterpret_cast<double *>(ws + L.partials);
+  unsigned *tickets = reinterpret_cast<unsigned *>(ws + L.tickets);
+  double *energies = reinterpret_cast<double *>(ws + L.energies);
+  const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((nthreads + kPmeBlock - 1) / kPmeBlock, sm_count() * 8));
+  pme_gather_kernel<T, Atoms, Out><<<nb, kPmeBlock, 0, s>>>(atoms, nthreads, box, p.K, phi_grid, alpha, out,
+                                                            partials, tickets + 1, energies + 1, energies, e_scale,
+                                                            energy_out);
+  TFF_LAUNCHED();
+  return TFF_OK;
+}
+
+}  // namespace tff

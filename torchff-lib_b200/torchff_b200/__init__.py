@@ -1,0 +1,25 @@
+"""torchff_b200: sm_100a implementation of torchff's fixed-charge nonbonded energy/force path.
+
+Importing the package loads libtffb200.so and registers the reference operator schemas
+under ``torch.ops.torchff``. Module classes keep the reference names and signatures:
+NeighborList, Nonbonded, Coulomb, Vdw, MultipolarInteraction (rank 0), PME (rank 0), PBC;
+FixedChargeSystem / FixedChargeNonbonded evaluate the whole nonbonded model in one call.
+"""
+from . import _lib  # noqa: F401  (fails loudly when the CUDA library is missing)
+from . import ops  # noqa: F401
+from .coulomb import Coulomb, compute_coulomb_energy
+from .multipoles import MultipolarInteraction, compute_multipolar_energy_from_atom_pairs
+from .nblist import NeighborList, build_neighbor_list_cell_list, build_neighbor_list_nsquared
+from .nonbonded import (Nonbonded, compute_nonbonded_energy_from_atom_pairs,
+                        compute_nonbonded_forces_from_atom_pairs)
+from .pbc import PBC, applyPBC
+from .pme import PME
+from .system import FixedChargeNonbonded, FixedChargeSystem
+from .vdw import Vdw, compute_lennard_jones_energy
+
+__all__ = [
+    "Coulomb", "compute_coulomb_energy", "MultipolarInteraction", "compute_multipolar_energy_from_atom_pairs",
+    "NeighborList", "build_neighbor_list_cell_list", "build_neighbor_list_nsquared", "Nonbonded",
+    "compute_nonbonded_energy_from_atom_pairs", "compute_nonbonded_forces_from_atom_pairs", "PBC", "applyPBC",
+    "PME", "FixedChargeNonbonded", "FixedChargeSystem", "Vdw", "compute_lennard_jones_energy",
+]

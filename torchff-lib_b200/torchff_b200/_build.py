@@ -1,0 +1,79 @@
+"""Builds libtffb200.so (sm_100a) from torchff-lib_b200/csrc with nvcc, in-tree.
+
+    python torchff-lib_b200/torchff_b200/_build.py [-f] [-v]
+
+Run as a script (not ``-m``): importing the package first would try to load the library.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG_DIR)                       # torchff-lib_b200/
+CSRC = os.path.join(ROOT, "csrc")
+INCLUDE = os.path.join(os.path.dirname(ROOT), "include")
+BUILD = os.path.join(ROOT, "_build")
+LIB_NAME = "libtffb200.so"
+SOURCES = ["tff_common.cu", "pairs.cu", "nblist.cu", "pme.cu", "fused.cu"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
+              "-Xptxas", "-warn-spills"]
+
+
+def nvcc() -> str:
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    p = os.path.join(cuda, "bin", "nvcc")
+    return p if os.path.exists(p) else (shutil.which("nvcc") or "nvcc")
+
+
+def lib_path() -> str:
+    return os.path.join(PKG_DIR, LIB_NAME)
+
+
+def _needs_rebuild(obj: str, deps: list[str]) -> bool:
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    headers.append(os.path.join(INCLUDE, "tffb200.h"))
+    objs = []
+    jobs = []
+    for src in SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        objs.append(o)
+        if force or _needs_rebuild(o, [s] + headers):
+            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o]
+            jobs.append(cmd)
+
+    def run(cmd):
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+        if verbose and (r.stdout or r.stderr):
+            print(r.stdout, r.stderr, file=sys.stderr)
+        return r
+
+    with cf.ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
+        list(ex.map(run, jobs))
+    out = lib_path()
+    if jobs or not os.path.exists(out) or force:
+        cuda = os.path.dirname(os.path.dirname(nvcc()))
+        link = [nvcc(), *ARCH, "-shared", "-o", out, *objs, "-cudart", "static", "-lcufft",
+                "-L", os.path.join(cuda, "lib64"), "-Xlinker", f"-rpath,{os.path.join(cuda, 'lib64')}"]
+        run(link)
+    return out
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -1,0 +1,194 @@
+"""Fused fixed-charge nonbonded evaluation of one periodic system.
+
+``FixedChargeSystem`` owns a libtffb200 system object: per-atom charges, Lennard-Jones
+sigma/epsilon (Lorentz-Berthelot combining), the exclusion list, a PME plan and all
+scratch, resident on the device. One ``evaluate`` call rebuilds the cluster-pair
+neighbour structure from the coordinates and returns the energy
+
+    E = sum_{pairs, r<=rc} [4 eps_ij((s_ij/r)^12 - (s_ij/r)^6) + k q_i q_j erfc(a r)/r]
+        - sum_{excluded pairs, r<=rc} k q_i q_j erf(a r)/r
+        + k E_pme(a, K)
+
+and forces, i.e. the nonbonded part of ``Tip3pTorchFF`` (examples/tip3p/model.py:100-133:
+NeighborList + Vdw + MultipolarInteraction(rank 0, pairs_excl) + 138.935456 * PME), with
+excluded pairs removed from the neighbour list and given the Ewald exclusion correction.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+import torch.nn as nn
+
+from . import _lib as L
+
+COULOMB_PREFACTOR = 138.935456
+
+
+class FixedChargeSystem:
+    def __init__(self, charges, sigma, epsilon, exclusions, cutoff: float, ewald_alpha: float, pme_grid: int,
+                 coul_constant: float = COULOMB_PREFACTOR, dtype: torch.dtype = torch.float32,
+                 device: torch.device | str = "cuda", max_cluster_neighbors: int = 0):
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise RuntimeError("FixedChargeSystem needs a CUDA device")
+        self.dtype = dtype
+        q = np.ascontiguousarray(np.asarray(charges, dtype=np.float64).reshape(-1))
+        s = np.ascontiguousarray(np.asarray(sigma, dtype=np.float64).reshape(-1))
+        e = np.ascontiguousarray(np.asarray(epsilon, dtype=np.float64).reshape(-1))
+        ex = np.ascontiguousarray(np.asarray(exclusions if exclusions is not None else np.zeros((0, 2)),
+                                             dtype=np.int64).reshape(-1, 2))
+        self.natoms = int(q.shape[0])
+        if s.shape[0] != self.natoms or e.shape[0] != self.natoms:
+            raise ValueError("charges, sigma and epsilon must all have natoms entries")
+        self.cutoff, self.ewald_alpha, self.pme_grid = float(cutoff), float(ewald_alpha), int(pme_grid)
+        self.coul_constant = float(coul_constant)
+        desc = L.SystemDesc(L.dtype_code(dtype), self.natoms, self.cutoff, self.ewald_alpha, self.pme_grid,
+                            self.coul_constant, int(max_cluster_neighbors))
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            L.check(L.lib.tff_system_create(ctypes.byref(desc), q.ctypes.data_as(ctypes.c_void_p),
+                                            s.ctypes.data_as(ctypes.c_void_p), e.ctypes.data_as(ctypes.c_void_p),
+                                            ex.shape[0], ex.ctypes.data_as(ctypes.c_void_p), ctypes.byref(h)),
+                    "tff_system_create")
+        self._h = h
+
+    @classmethod
+    def from_water_box(cls, wb, dtype=torch.float32, device="cuda", **kw):
+        """System for a ``torchff_b200.water.WaterBox`` (TIP3P parameters and exclusions)."""
+        return cls(wb.charges, wb.sigma, wb.epsilon, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
+                   dtype=dtype, device=device, **kw)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                L.lib.tff_system_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def set_parameters(self, charges=None, sigma=None, epsilon=None) -> None:
+        ts = [None if t is None else t.detach().to(self.device, self.dtype).contiguous() for t in
+              (charges, sigma, epsilon)]
+        L.check(L.lib.tff_system_set_parameters(self._h, *(L.ptr(t) for t in ts), self._stream()),
+                "tff_system_set_parameters")
+
+    def evaluate_into(self, coords: torch.Tensor, box: torch.Tensor, energy: torch.Tensor, forces: torch.Tensor,
+                      grad_charges: torch.Tensor | None = None, energy_terms: torch.Tensor | None = None) -> None:
+        """Enqueues one evaluation writing into preallocated outputs (CUDA-graph friendly).
+
+        coords (N,3) and box (3,3) in the system dtype; energy: float64 (1,); forces (N,3)
+        system dtype (= -dE/dx); grad_charges (N,) dE/dq; energy_terms float64 (4,):
+        real-space pairs, exclusion correction, reciprocal, self.
+        """
+        L.check(L.lib.tff_system_eval(self._h, L.ptr(coords), L.ptr(box), L.ptr(energy), L.ptr(forces),
+                                      L.ptr(grad_charges), L.ptr(energy_terms), self._stream()), "tff_system_eval")
+
+    def evaluate(self, coords: torch.Tensor, box: torch.Tensor, grad_charges: bool = False, terms: bool = False):
+        x = coords.detach().to(self.device, self.dtype).contiguous()
+        b = box.detach().to(self.device, self.dtype).contiguous()
+        if x.shape != (self.natoms, 3):
+            raise ValueError(f"coords must be ({self.natoms}, 3)")
+        energy = torch.empty(1, dtype=torch.float64, device=self.device)
+        forces = torch.empty_like(x)
+        gq = torch.empty(self.natoms, dtype=self.dtype, device=self.device) if grad_charges else None
+        et = torch.empty(4, dtype=torch.float64, device=self.device) if terms else None
+        self.evaluate_into(x, b, energy, forces, gq, et)
+        out = {"energy": energy[0], "forces": forces}
+        if gq is not None:
+            out["grad_charges"] = gq
+        if et is not None:
+            out["terms"] = et
+        return out
+
+    def evaluate_host(self, coords: np.ndarray | torch.Tensor, box: np.ndarray | torch.Tensor,
+                      forces_out: np.ndarray | torch.Tensor) -> float:
+        """Host buffers in and out (float64): H2D copy, evaluation, D2H copy, synchronise."""
+        e = ctypes.c_double(0.0)
+        cp = coords.data_ptr() if isinstance(coords, torch.Tensor) else coords.ctypes.data
+        bp = box.data_ptr() if isinstance(box, torch.Tensor) else box.ctypes.data
+        fp = forces_out.data_ptr() if isinstance(forces_out, torch.Tensor) else forces_out.ctypes.data
+        L.check(L.lib.tff_system_eval_host(self._h, ctypes.c_void_p(cp), ctypes.c_void_p(bp), ctypes.byref(e),
+                                           ctypes.c_void_p(fp), self._stream()), "tff_system_eval_host")
+        return e.value
+
+    def status(self) -> int:
+        v = ctypes.c_int(0)
+        L.check(L.lib.tff_system_status(self._h, self._stream(), ctypes.byref(v)), "tff_system_status")
+        return v.value
+
+    def kernel_launches(self) -> int:
+        """Kernels of libtffb200 one evaluation launches (cuFFT's not counted)."""
+        return int(L.lib.tff_system_kernel_launches(self._h))
+
+    def evaluate_timed_into(self, coords, box, energy, forces, timer: "StageTimer") -> None:
+        """Like evaluate_into, recording the stage events of ``timer`` (graph-capturable)."""
+        L.check(L.lib.tff_system_eval_timed(self._h, L.ptr(coords), L.ptr(box), L.ptr(energy), L.ptr(forces),
+                                            timer.handle, self._stream()), "tff_system_eval_timed")
+
+
+class StageTimer:
+    """CUDA events at the stage boundaries of a fused evaluation.
+
+    Event k: 0 start, 1 cluster build, 2 real-space tile kernel, 3 PME grid phase
+    (spread, FFTs, influence function), 4 PME gather, 5 finalize.
+    """
+
+    STAGES = ("cluster_build", "tile_kernel", "pme_grid", "pme_gather", "finalize")
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        L.check(L.lib.tff_timer_create(ctypes.byref(h)), "tff_timer_create")
+        self.handle = h
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        v = ctypes.c_float(0.0)
+        L.check(L.lib.tff_timer_elapsed_ms(self.handle, a, b, ctypes.byref(v)), "tff_timer_elapsed_ms")
+        return float(v.value)
+
+    def stages_ms(self) -> dict:
+        return {name: self.elapsed_ms(k, k + 1) for k, name in enumerate(self.STAGES)}
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                L.lib.tff_timer_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+
+class _SystemEnergyFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coords, box, charges, system: FixedChargeSystem):
+        out = system.evaluate(coords, box, grad_charges=ctx.needs_input_grad[2])
+        ctx.save_for_backward(out["forces"], out.get("grad_charges"))
+        return out["energy"].to(coords.dtype)
+
+    @staticmethod
+    def backward(ctx, g):
+        f, gq = ctx.saved_tensors
+        return -f * g, None, (None if gq is None else gq * g), None
+
+
+class FixedChargeNonbonded(nn.Module):
+    """nn.Module view of a FixedChargeSystem: ``forward(coords, box) -> E`` with forces via autograd.
+
+    ``charges`` passed to forward (optional) must equal the system's charges; it is
+    accepted so that dE/dq flows to a leaf tensor.
+    """
+
+    def __init__(self, system: FixedChargeSystem):
+        super().__init__()
+        self.system = system
+
+    def forward(self, coords: torch.Tensor, box: torch.Tensor, charges: torch.Tensor | None = None):
+        if charges is not None:
+            self.system.set_parameters(charges=charges)
+        return _SystemEnergyFn.apply(coords, box, charges, self.system)
