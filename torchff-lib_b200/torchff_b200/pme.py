@@ -29,9 +29,11 @@ class PME(nn.Module):
         self.use_customized_ops = use_customized_ops
         self.return_fields = return_fields
         K = self.max_hkl
-        self.register_buffer("xmoduli", bsplines.compute_bspline_moduli_1d(K, dtype=torch.float32))
-        self.register_buffer("ymoduli", bsplines.compute_bspline_moduli_1d(K, dtype=torch.float32))
-        self.register_buffer("zmoduli", bsplines.compute_bspline_moduli_z(K, dtype=torch.float32))
+        # float64 moduli (the reference registers float32 ones, torchff/pme.py:21-28, which
+        # limits its FP64 path to ~1e-7 relative); .to(float32) still casts them down.
+        self.register_buffer("xmoduli", bsplines.compute_bspline_moduli_1d(K, dtype=torch.float64))
+        self.register_buffer("ymoduli", bsplines.compute_bspline_moduli_1d(K, dtype=torch.float64))
+        self.register_buffer("zmoduli", bsplines.compute_bspline_moduli_z(K, dtype=torch.float64))
 
     @torch._dynamo.disable
     def forward(self, coords: torch.Tensor, box: torch.Tensor, q: torch.Tensor, p: Optional[torch.Tensor] = None,
