@@ -101,6 +101,25 @@ int tff_nonbonded_atom_pairs(int dtype, int64_t natoms, const void *coords, int6
                              void *grad_sigma, void *grad_epsilon, void *grad_charges,
                              void *workspace, size_t workspace_bytes, tff_stream_t stream);
 
+/* No counterpart in the reference. tff_nonbonded_atom_pairs without a workspace, for
+ * callers that cannot allocate device memory: a plugin whose host engine owns every device
+ * allocation, work enqueued while a stream capture forbids allocating, or a loop that must
+ * not reach an allocator. This entry point calls no cudaMalloc/cudaFree and no allocating
+ * library routine; its scratch is a static device array inside libtffb200 (about 3 MiB,
+ * held by every GPU that loads the library until exit), so natoms is limited to
+ * TFF_NOALLOC_MAX_ATOMS (larger inputs return TFF_ERR_INVALID). The first call on each
+ * device looks the array up with cudaGetSymbolAddress: make it before any stream capture.
+ * All calls share the array (cleared at the start of each call, it keeps the last call's
+ * contents): calls that overlap on the GPU race, so serialise them. Inputs, outputs and
+ * results are those of tff_nonbonded_atom_pairs. */
+#define TFF_NOALLOC_MAX_ATOMS 65536
+int tff_nonbonded_atom_pairs_noalloc(int dtype, int64_t natoms, const void *coords,
+                                     int64_t npairs, const int64_t *pairs, const void *box,
+                                     const void *sigma, const void *epsilon, const void *charges,
+                                     double coul_constant, double cutoff, int do_shift,
+                                     void *energy, void *grad_coords, void *grad_sigma,
+                                     void *grad_epsilon, void *grad_charges, tff_stream_t stream);
+
 /* Replaces torch.ops.torchff.compute_nonbonded_forces_from_atom_pairs
  * (csrc/nonbonded/nonbonded_interface.cpp:10, csrc/nonbonded/nonbonded_atom_pairs_cuda.cu:263-305):
  * ADDS the shifted Coulomb + LJ forces -dE/dx into `forces` (N,3). */

@@ -10,6 +10,8 @@
 // atomics in FP64 mode.
 #include <math.h>
 
+#include <mutex>
+
 #include "tff_common.cuh"
 
 namespace tff {
@@ -343,12 +345,78 @@ int run_pairs_any(const PairCall &c, cudaStream_t s) {
   return c.dtype == TFF_F32 ? run_pairs<float>(c, s) : run_pairs<double>(c, s);
 }
 
+// ---------------------------------------------------------------------------------------
+// Scratch for tff_nonbonded_atom_pairs_noalloc: a file-scope device array, so that caller
+// never has to allocate. Sized for TFF_NOALLOC_MAX_ATOMS atoms (6 accumulators of 8 bytes
+// per atom, the block partials and the reduction ticket/energy); every GPU that loads the
+// library holds it until the process exits.
+// ---------------------------------------------------------------------------------------
+constexpr int64_t kNoAllocMaxAtoms = TFF_NOALLOC_MAX_ATOMS;
+constexpr size_t kNoAllocScratchBytes = (size_t)kNoAllocMaxAtoms * 6 * 8 + 8192 * 8 + 512;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch on the current device. In host code the symbol is
+// only a host-side stand-in, so the address is looked up once per device with
+// cudaGetSymbolAddress (with that device current) and cached.
+int noalloc_scratch(void **out) {
+  static std::mutex mu;
+  static void *addr[64] = {nullptr};
+  int dev = 0;
+  TFF_CUDA(cudaGetDevice(&dev));
+  TFF_ARG(dev >= 0 && dev < 64, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (addr[dev] == nullptr) {
+    void *p = nullptr;
+    TFF_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    addr[dev] = p;
+  }
+  *out = addr[dev];
+  return TFF_OK;
+}
+
 }  // namespace
 }  // namespace tff
 
 using namespace tff;
 
 extern "C" {
+
+// Same computation as tff_nonbonded_atom_pairs, for callers that cannot allocate device
+// memory: a plugin running inside a host engine that owns every device allocation, code
+// that enqueues work while a CUDA stream capture forbids allocation, or a loop that must
+// never reach an allocator. Scratch is the library's static device array instead of a
+// caller workspace; the caller still passes inputs and outputs. Limits and sharing:
+// natoms <= TFF_NOALLOC_MAX_ATOMS (larger sizes return TFF_ERR_INVALID); the first call on
+// each device looks the array up with cudaGetSymbolAddress, so make that first call before
+// any stream capture; all calls share the one array (its accumulators are cleared at the
+// start of every call and it keeps the last call's contents), so calls that overlap on the
+// GPU, e.g. on two streams at once, race and must be serialised by the caller.
+int tff_nonbonded_atom_pairs_noalloc(int dtype, int64_t natoms, const void *coords, int64_t npairs,
+                                     const int64_t *pairs, const void *box, const void *sigma,
+                                     const void *epsilon, const void *charges, double coul_constant,
+                                     double cutoff, int do_shift, void *energy, void *grad_coords,
+                                     void *grad_sigma, void *grad_epsilon, void *grad_charges,
+                                     tff_stream_t stream) {
+  TFF_ARG(natoms >= 0 && natoms <= kNoAllocMaxAtoms,
+          "natoms=%lld exceeds the static scratch limit of %lld atoms of tff_nonbonded_atom_pairs_noalloc",
+          (long long)natoms, (long long)kNoAllocMaxAtoms);
+  const size_t need = pair_layout(dtype, natoms, 0).bytes;
+  TFF_ARG(need <= kNoAllocScratchBytes, "static scratch too small (%zu > %zu bytes)", need, kNoAllocScratchBytes);
+  void *ws = nullptr;
+  int st = noalloc_scratch(&ws);
+  if (st != TFF_OK) return st;
+  PairCall c{};
+  c.dtype = dtype;
+  c.cm = do_shift ? C_SHIFT : C_PLAIN;
+  c.lm = L_ATOM;
+  c.natoms = natoms; c.npairs = npairs; c.x = coords; c.box = box; c.q = charges;
+  c.sig = sigma; c.eps = epsilon; c.pairs = pairs; c.k = coul_constant; c.rc = cutoff;
+  c.energy = energy; c.e_scale = 1.0;
+  c.gx = grad_coords; c.gx_scale = 1.0; c.gx_add = false;
+  c.gq = grad_charges; c.gs = grad_sigma; c.ge = grad_epsilon;
+  c.ws = ws; c.ws_bytes = kNoAllocScratchBytes;
+  return run_pairs_any(c, (cudaStream_t)stream);
+}
 
 size_t tff_pairs_workspace_bytes(int dtype, int64_t natoms, int64_t ntypes) {
   return pair_layout(dtype, natoms, ntypes).bytes;

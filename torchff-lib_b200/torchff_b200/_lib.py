@@ -42,7 +42,9 @@ _SIGS = {
     "tff_pairs_workspace_bytes": (sz, [i32, i64, i64]),
     "tff_nonbonded_atom_pairs": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, f64, f64, i32, vp, vp, vp, vp, vp,
                                        vp, sz, vp]),
-    "tff_nonbonded_forces_atom_pairs": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, f64, f64, vp, vp, sz, vp]),
+    "tff_nonbonded_atom_pairs_noalloc": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, f64, f64, i32, vp, vp, vp,
+                                               vp, vp, vp]),
+    "tff_nonbonded_forces_atom_pairs":(i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, f64, f64, vp, vp, sz, vp]),
     "tff_coulomb_atom_pairs": (i32, [i32, i64, vp, i64, vp, vp, vp, f64, f64, i32, vp, vp, vp, vp, sz, vp]),
     "tff_lennard_jones_atom_pairs": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, f64, vp, i64, vp, vp, vp, vp, vp,
                                            sz, vp]),
