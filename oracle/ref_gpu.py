@@ -1,0 +1,185 @@
+"""The reference's own CUDA operators on the GPU: timing baseline and an oracle cross-check.
+
+TEST/MEASUREMENT INFRASTRUCTURE. Loads the reference's compiled extension libraries from
+``oracle/_ref`` (built by ``oracle/build_ref.py``). These register ``torch.ops.torchff``
+exactly like torchff_b200 does, so this script always runs in a process of its own.
+
+It evaluates the nonbonded part of the reference's TIP3P model
+(``examples/tip3p/model.py:100-133``): ``build_neighbor_list_cell_list`` with the water
+exclusions, ``compute_lennard_jones_energy`` with type tables,
+``compute_multipolar_energy_from_atom_pairs`` (rank 0, Ewald, ``pairs_excl``) and
+138.935456 x ``pme_long_range``, energy + backward. Timing follows the reference's
+``perf_op`` (``torchff/test_utils.py:52-146``): warm-up, then forward + backward captured in
+one CUDA graph and replayed. Prints one JSON line per precision.
+
+    python oracle/ref_gpu.py [--workload water3000] [--steps 200] [--check]
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import json
+import math
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+sys.path.insert(0, REPO)
+
+
+def water_module():
+    """torchff_b200/water.py loaded by path: importing the torchff_b200 package would
+    register its own torch.ops.torchff schemas, which clash with the reference's."""
+    import importlib.util
+
+    path = os.path.join(REPO, "torchff-lib_b200", "torchff_b200", "water.py")
+    spec = importlib.util.spec_from_file_location("_tff_water", path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["_tff_water"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_reference_ops() -> list[str]:
+    import torch
+
+    libs = sorted(glob.glob(os.path.join(HERE, "_ref", "*", "*.so")))
+    if not libs:
+        raise SystemExit("oracle/_ref has no reference libraries (run oracle/build_ref.py)")
+    for lib in libs:
+        torch.ops.load_library(lib)
+    return libs
+
+
+def moduli(K: int, dtype):
+    """B-spline moduli with the reference's float32 buffers (torchff/pme.py:21-28)."""
+    import torch
+
+    m = [0.0, 1.0 / 120, 26.0 / 120, 66.0 / 120, 26.0 / 120, 1.0 / 120]
+
+    def mod(count):
+        k = torch.arange(count, dtype=torch.float64)
+        out = torch.zeros(count, dtype=torch.float64)
+        for j in range(-3, 3):
+            out += m[j + 3] * torch.cos(2 * math.pi * j * k / K)
+        return out.to(torch.float32).to(dtype).cuda()
+
+    return mod(K), mod(K), mod(K // 2 + 1)
+
+
+def build_inputs(wb, dtype):
+    import torch
+
+    from oracle import oracle as O
+
+    dev = "cuda"
+    rp, col = (torch.tensor(a, device=dev) for a in O.exclusions_coo_to_csr(wb.nblist_exclusions, wb.natoms))
+    return {
+        "coords": torch.tensor(wb.coords, dtype=dtype, device=dev, requires_grad=True),
+        "box": torch.tensor(wb.box, dtype=dtype, device=dev),
+        "q": torch.tensor(wb.charges, dtype=dtype, device=dev),
+        "sig": torch.tensor(wb.sigma_table, dtype=dtype, device=dev),
+        "eps": torch.tensor(wb.epsilon_table, dtype=dtype, device=dev),
+        "types": torch.tensor(wb.atom_types, dtype=torch.int64, device=dev),
+        "excl": torch.tensor(wb.coulomb_exclusions, dtype=torch.int64, device=dev),
+        "rp": rp, "col": col,
+        "mod": moduli(wb.grid, dtype),
+        "cap": int(wb.natoms * 4 / 3 * 3.1416 * wb.cutoff ** 3 * 100 / 2 * 1.2),
+    }
+
+
+def energy(wb, d):
+    import torch
+
+    ops = torch.ops.torchff
+    x, b = d["coords"], d["box"]
+    pairs, _ = ops.build_neighbor_list_cell_list(x.detach(), b, wb.cutoff, d["cap"], d["rp"], d["col"], False)
+    e_lj = ops.compute_lennard_jones_energy(x, pairs, b, d["sig"], d["eps"], wb.cutoff, d["types"])
+    e_c = ops.compute_multipolar_energy_from_atom_pairs(x, b, pairs, d["excl"], d["q"], None, None, wb.cutoff,
+                                                         wb.alpha, 138.935456)
+    e_p = ops.pme_long_range(x, b, d["q"], None, None, wb.grid, wb.alpha, *d["mod"]) * 138.935456
+    return e_lj + e_c + e_p
+
+
+def time_graph(wb, d, steps: int, warmup: int = 5) -> tuple[float, str]:
+    """ms per forward + backward: CUDA-graph replay as in torchff/test_utils.py:52-146, or,
+    when the composition cannot be captured, back-to-back eager calls."""
+    import torch
+
+    x = d["coords"]
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(warmup):
+            x.grad = None
+            energy(wb, d).backward()
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    mode = "cuda_graph"
+    try:
+        g = torch.cuda.CUDAGraph()
+        x.grad = None
+        with torch.cuda.graph(g):
+            e = energy(wb, d)
+            e.backward()
+        for _ in range(warmup):
+            g.replay()
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(steps):
+            g.replay()
+        z.record()
+    except Exception:  # capture invalidated by a host synchronisation inside an op
+        mode = "eager"
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(steps):
+            x.grad = None
+            energy(wb, d).backward()
+        z.record()
+    z.synchronize()
+    return a.elapsed_time(z) / steps, mode
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="water3000", choices=["water216", "water3000"])
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--check", action="store_true", help="compare the FP64 energy/forces with the oracle")
+    args = ap.parse_args()
+    import numpy as np
+    import torch
+
+    W = water_module()
+    load_reference_ops()
+    wb = {"water216": W.water_box_216, "water3000": W.water_box_3000}[args.workload](0)
+    out = {"workload": args.workload, "natoms": wb.natoms}
+    for name, dtype in (("fp64", torch.float64), ("fp32", torch.float32)):
+        d = build_inputs(wb, dtype)
+        e = energy(wb, d)
+        e.backward()
+        out[f"{name}_energy"] = float(e.item())
+        out[f"{name}_forces"] = (-d["coords"].grad).double().cpu().numpy()
+        out[f"{name}_ms_per_eval"], out[f"{name}_timing_mode"] = time_graph(wb, d, args.steps)
+        out[f"{name}_evals_per_s"] = 1e3 / out[f"{name}_ms_per_eval"]
+    if args.check:
+        from oracle import oracle as O
+
+        ref = O.fixed_charge_energy(wb.coords, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
+                                    wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
+                                    138.935456)
+        f0 = -ref["grad_coords"]
+        for name in ("fp64", "fp32"):
+            f = out[f"{name}_forces"]
+            out[f"{name}_energy_rel_err_vs_oracle"] = abs(out[f"{name}_energy"] - ref["total"]) / abs(ref["total"])
+            out[f"{name}_force_rel_rms_vs_oracle"] = float(np.sqrt(np.mean((f - f0) ** 2)) / np.sqrt(np.mean(f0 ** 2)))
+        out["oracle_energy"] = ref["total"]
+    for name in ("fp64", "fp32"):
+        out.pop(f"{name}_forces")
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

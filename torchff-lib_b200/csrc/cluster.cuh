@@ -1,10 +1,10 @@
 // Cluster build shared by the cell-list neighbour list and the fused real-space kernel.
 //
 // 1. cell_keys:      fractional coordinates wrapped to [0,1), cell on an nc^3 grid
-//                    (about 4 atoms per cell), Morton key, per-key histogram.
-// 2. scan_keys:      exclusive scan of the histogram (one block).
+//                    (about 8 atoms per cell), Morton key, per-key histogram.
+// 2. scan_keys:      exclusive scan of the histogram (one block, segmented).
 // 3. scatter_atoms:  atoms into key buckets (slot order inside a bucket is arbitrary).
-// 4. sort_buckets:   each bucket sorted by atom index -> deterministic order; writes the
+// 4. sort_buckets:   one warp per bucket ranks its atoms by index -> deterministic order; writes the
 //                    sorted SoA (wrapped position + charge as a 4-vector, original index,
 //                    inverse map, fractional position) and pads to a multiple of 32.
 // 5. cluster_bounds: one warp per 32-atom cluster: fractional bounding box.
@@ -12,13 +12,19 @@
 //                    those whose boxes can hold a pair within the cutoff (order of the
 //                    list is deterministic). `half` keeps only J <= I.
 //
-// The Morton order of ~4-atom cells makes 32 consecutive atoms a compact blob (about a
-// 2x2x2 block of cells), which is what the 32x32 warp tiles need.
+// The Morton order of ~8-atom cells makes 32 consecutive atoms a compact blob (a 2x2x1
+// block of cells), which is what the 32x32 warp tiles need.
 #pragma once
+
+#include <climits>
 
 #include "tff_common.cuh"
 
 namespace tff {
+
+// Neighbour clusters per tile-kernel work item (a work item is one cluster I and every
+// (ncount/kItemTiles)-th cluster of its list).
+constexpr int kItemTiles = 8;
 
 template <class T> struct V4;
 template <> struct V4<float> { using type = float4; };
@@ -32,23 +38,16 @@ struct ClusterLayout {
   int nc = 1, bits = 0;
   int64_t nkeys = 1, natoms = 0, nclusters = 0, npad = 0;
   int cap = 0;
-  size_t keys, hist, fill, status, tmp, sidx, inv, pos, frac, bc, bh, nbr, ncount, boxinfo;
+  size_t keys, hist, fill, status, tmp, sidx, inv, pos, frac, bc, bh, nbr, ncount, itemoff, items, boxinfo;
   size_t zero_off, zero_bytes, bytes;
 };
-
-inline unsigned morton_spread_host(unsigned v) {
-  v &= 0x3ff;
-  v = (v | (v << 16)) & 0x030000FF;
-  v = (v | (v << 8)) & 0x0300F00F;
-  v = (v | (v << 4)) & 0x030C30C3;
-  v = (v | (v << 2)) & 0x09249249;
-  return v;
-}
 
 inline ClusterLayout cluster_layout(int dtype, int64_t natoms, int cap) {
   ClusterLayout L;
   L.natoms = natoms;
-  int nc = (int)floor(cbrt((double)natoms / 4.0));
+  // ~8 atoms per cell: with Morton order, runs of 32 atoms form the most compact clusters
+  // (fewest cluster pairs within the cutoff) among 2..32 atoms per cell on water boxes
+  int nc = (int)floor(cbrt((double)natoms / 8.0));
   nc = std::max(1, std::min(nc, 128));
   int bits = 0;
   while ((1 << bits) < nc) ++bits;
@@ -76,6 +75,8 @@ inline ClusterLayout cluster_layout(int dtype, int64_t natoms, int cap) {
   L.bh = (c.off + 255) & ~size_t(255); c.take<char>(L.nclusters * 4 * tsz);
   L.nbr = (c.off + 255) & ~size_t(255); c.take<int>((size_t)L.nclusters * cap);
   L.ncount = (c.off + 255) & ~size_t(255); c.take<int>(L.nclusters);
+  L.itemoff = (c.off + 255) & ~size_t(255); c.take<int>(L.nclusters + 1);
+  L.items = (c.off + 255) & ~size_t(255); c.take<int>((size_t)L.nclusters * ((cap + kItemTiles - 1) / kItemTiles));
   L.boxinfo = (c.off + 255) & ~size_t(255); c.take<double>(32);
   L.bytes = c.bytes();
   return L;
@@ -87,6 +88,8 @@ struct ClusterData {
   using V = typename V4<T>::type;
   unsigned *keys, *hist, *fill, *status;
   int *tmp, *sidx, *inv, *nbr, *ncount;
+  int *itemoff;  // work items of the tile kernel: prefix sums of ceil(ncount / kItemTiles)
+  int *items;    // owning cluster of each work item
   V *pos, *frac, *bc, *bh;
   double *boxinfo;  // [0..8] box, [9..17] inv, [18] ortho flag, [19..21] perpendicular widths
   int nc, bits, cap;
@@ -107,6 +110,8 @@ inline ClusterData<T> cluster_data(const ClusterLayout &L, void *ws) {
   d.inv = reinterpret_cast<int *>(b + L.inv);
   d.nbr = reinterpret_cast<int *>(b + L.nbr);
   d.ncount = reinterpret_cast<int *>(b + L.ncount);
+  d.itemoff = reinterpret_cast<int *>(b + L.itemoff);
+  d.items = reinterpret_cast<int *>(b + L.items);
   d.pos = reinterpret_cast<V *>(b + L.pos);
   d.frac = reinterpret_cast<V *>(b + L.frac);
   d.bc = reinterpret_cast<V *>(b + L.bc);
@@ -175,42 +180,42 @@ __global__ void cell_keys_kernel(const T *x, int64_t n, ClusterData<T> d) {
   }
 }
 
-// Exclusive scan of hist[0..nkeys) in place; hist[nkeys] = total. One block of 1024.
+// Exclusive scan of hist[0..nkeys) in place; hist[nkeys] = total. One block of 1024
+// threads; thread t owns a contiguous segment, so the work is two sweeps of the segment
+// plus one block-wide scan of the segment sums.
 static __global__ void scan_keys_kernel(unsigned *hist, int64_t nkeys) {
   __shared__ unsigned s_warp[32];
-  __shared__ unsigned s_carry;
-  if (threadIdx.x == 0) s_carry = 0;
-  __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int64_t base = 0; base < nkeys; base += blockDim.x) {
-    int64_t k = base + threadIdx.x;
-    unsigned v = (k < nkeys) ? hist[k] : 0u;
-    unsigned incl = v;
+  const int64_t per = (nkeys + blockDim.x - 1) / blockDim.x;
+  const int64_t beg = min((int64_t)threadIdx.x * per, nkeys), end = min(beg + per, nkeys);
+  unsigned sum = 0;
+  for (int64_t k = beg; k < end; ++k) sum += hist[k];
+  unsigned incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_warp[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    const unsigned t = (lane < (int)(blockDim.x >> 5)) ? s_warp[lane] : 0u;
+    unsigned ti = t;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      unsigned y = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += y;
+      const unsigned y = __shfl_up_sync(kFull, ti, o);
+      if (lane >= o) ti += y;
     }
-    if (lane == 31) s_warp[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-      unsigned t = (lane < (int)(blockDim.x >> 5)) ? s_warp[lane] : 0u;
-      unsigned ti = t;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        unsigned y = __shfl_up_sync(kFull, ti, o);
-        if (lane >= o) ti += y;
-      }
-      s_warp[lane] = ti - t;  // exclusive warp offsets
-    }
-    __syncthreads();
-    unsigned carry = s_carry;
-    if (k < nkeys) hist[k] = carry + s_warp[w] + incl - v;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) s_carry = carry + s_warp[w] + incl;
-    __syncthreads();
+    s_warp[lane] = ti - t;  // exclusive warp offsets
   }
-  if (threadIdx.x == 0) hist[nkeys] = s_carry;
+  __syncthreads();
+  unsigned run = s_warp[w] + incl - sum;
+  for (int64_t k = beg; k < end; ++k) {
+    const unsigned v = hist[k];
+    hist[k] = run;
+    run += v;
+  }
+  if (threadIdx.x == blockDim.x - 1) hist[nkeys] = run;
 }
 
 template <class T>
@@ -223,45 +228,49 @@ __global__ void scatter_atoms_kernel(int64_t n, ClusterData<T> d) {
   }
 }
 
-// One thread per key: insertion-sort the bucket by atom index, then write the sorted SoA.
-// q may be NULL (charge slot = 0).
+// One warp per key bucket: each atom's slot is its rank (by atom index) inside the bucket,
+// found by warp-wide counting, which gives a deterministic order with no serial chain;
+// then the sorted SoA is written. q may be NULL (charge slot = 0).
 template <class T>
 __global__ void sort_buckets_kernel(const T *x, const T *q, int64_t nkeys, ClusterData<T> d) {
   const double *m = d.boxinfo;
   const double *inv = d.boxinfo + 9;
-  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nkeys; k += gstride) {
-    const unsigned b0 = d.hist[k], b1 = d.hist[k + 1];
-    for (unsigned a = b0 + 1; a < b1; ++a) {
-      int v = d.tmp[a];
-      unsigned c = a;
-      while (c > b0 && d.tmp[c - 1] > v) {
-        d.tmp[c] = d.tmp[c - 1];
-        --c;
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t k = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); k < nkeys; k += nw) {
+    const unsigned b0 = d.hist[k], cnt = d.hist[k + 1] - b0;
+    for (unsigned base = 0; base < cnt; base += kWarp) {
+      const bool has = base + lane < cnt;
+      const int v = has ? d.tmp[b0 + base + lane] : INT_MAX;
+      unsigned rank = 0;
+      for (unsigned cb = 0; cb < cnt; cb += kWarp) {
+        const int other = (cb + lane < cnt) ? d.tmp[b0 + cb + lane] : INT_MAX;
+#pragma unroll 8
+        for (int s = 0; s < kWarp; ++s) rank += (__shfl_sync(kFull, other, s) < v) ? 1u : 0u;
       }
-      d.tmp[c] = v;
-    }
-    for (unsigned s = b0; s < b1; ++s) {
-      const int i = d.tmp[s];
-      double rx = x[3 * i], ry = x[3 * i + 1], rz = x[3 * i + 2];
-      double f[3];
+      if (has) {
+        const unsigned slot = b0 + rank;
+        const double rx = x[3 * v], ry = x[3 * v + 1], rz = x[3 * v + 2];
+        double f[3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        double v = rx * inv[c] + ry * inv[3 + c] + rz * inv[6 + c];
-        v -= floor(v);
-        if (v >= 1.0) v = 0.0;
-        f[c] = v;
+        for (int c = 0; c < 3; ++c) {
+          double w = rx * inv[c] + ry * inv[3 + c] + rz * inv[6 + c];
+          w -= floor(w);
+          if (w >= 1.0) w = 0.0;
+          f[c] = w;
+        }
+        const double wx = f[0] * m[0] + f[1] * m[3] + f[2] * m[6];
+        const double wy = f[0] * m[1] + f[1] * m[4] + f[2] * m[7];
+        const double wz = f[0] * m[2] + f[1] * m[5] + f[2] * m[8];
+        d.pos[slot] = make_v4((T)wx, (T)wy, (T)wz, q ? q[v] : T(0));
+        d.frac[slot] = make_v4((T)f[0], (T)f[1], (T)f[2], T(0));
+        d.sidx[slot] = v;
+        d.inv[v] = (int)slot;
       }
-      double wx = f[0] * m[0] + f[1] * m[3] + f[2] * m[6];
-      double wy = f[0] * m[1] + f[1] * m[4] + f[2] * m[7];
-      double wz = f[0] * m[2] + f[1] * m[5] + f[2] * m[8];
-      d.pos[s] = make_v4((T)wx, (T)wy, (T)wz, q ? q[i] : T(0));
-      d.frac[s] = make_v4((T)f[0], (T)f[1], (T)f[2], T(0));
-      d.sidx[s] = i;
-      d.inv[i] = (int)s;
     }
   }
   // padding slots
+  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t s = d.natoms + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < d.npad; s += gstride) {
     d.sidx[s] = -1;
     d.pos[s] = make_v4(T(0), T(0), T(0), T(0));
@@ -270,11 +279,14 @@ __global__ void sort_buckets_kernel(const T *x, const T *q, int64_t nkeys, Clust
 }
 
 // One warp per cluster: bounding box in fractional coordinates. The box is taken around
-// the first atom's image so that a cluster straddling the periodic boundary stays compact.
+// the first atom's image so that a cluster straddling the periodic boundary stays compact,
+// and the cluster's positions are rewritten as that same contiguous image (anchor +
+// nearest-image offset), so that one periodic shift serves a whole cluster pair.
 template <class T>
 __global__ void cluster_bounds_kernel(ClusterData<T> d) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const double *m = d.boxinfo;
   for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < d.nclusters; c += nw) {
     const int64_t s = c * kWarp + lane;
     const bool valid = d.sidx[s] >= 0;
@@ -283,6 +295,14 @@ __global__ void cluster_bounds_kernel(ClusterData<T> d) {
     const T ax = __shfl_sync(kFull, fx, 0), ay = __shfl_sync(kFull, fy, 0), az = __shfl_sync(kFull, fz, 0);
     fx -= ax; fy -= ay; fz -= az;
     fx -= floor(fx + T(0.5)); fy -= floor(fy + T(0.5)); fz -= floor(fz + T(0.5));
+    if (valid) {
+      const double ux = (double)ax + (double)fx, uy = (double)ay + (double)fy, uz = (double)az + (double)fz;
+      auto p = d.pos[s];
+      p.x = (T)(ux * m[0] + uy * m[3] + uz * m[6]);
+      p.y = (T)(ux * m[1] + uy * m[4] + uz * m[7]);
+      p.z = (T)(ux * m[2] + uy * m[5] + uz * m[8]);
+      d.pos[s] = p;
+    }
     T lo[3] = {valid ? fx : T(1e30), valid ? fy : T(1e30), valid ? fz : T(1e30)};
     T hi[3] = {valid ? fx : T(-1e30), valid ? fy : T(-1e30), valid ? fz : T(-1e30)};
 #pragma unroll
@@ -351,6 +371,51 @@ __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) 
       if (count > d.cap) atomicOr(&d.status[0], 1u);
     }
   }
+  // The last block to finish turns the counts into work-item offsets (exclusive prefix
+  // sums of ceil(count / kItemTiles)); status[1] is the block ticket (zeroed per build).
+  __shared__ bool s_last;
+  __shared__ int s_warp[32];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&d.status[1], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const int64_t n = d.nclusters;
+  const int64_t per = (n + blockDim.x - 1) / blockDim.x;
+  const int64_t beg = min((int64_t)threadIdx.x * per, n), end = min(beg + per, n);
+  int sum = 0;
+  for (int64_t k = beg; k < end; ++k) sum += (__ldcg(&d.ncount[k]) + kItemTiles - 1) / kItemTiles;
+  int incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int w = threadIdx.x >> 5;
+  if (lane == 31) s_warp[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    const int t = (lane < (int)(blockDim.x >> 5)) ? s_warp[lane] : 0;
+    int ti = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, ti, o);
+      if (lane >= o) ti += y;
+    }
+    s_warp[lane] = ti - t;
+  }
+  __syncthreads();
+  int run = s_warp[w] + incl - sum;
+  for (int64_t k = beg; k < end; ++k) {
+    d.itemoff[k] = run;
+    const int nk = (__ldcg(&d.ncount[k]) + kItemTiles - 1) / kItemTiles;
+    for (int j = 0; j < nk; ++j) d.items[run + j] = (int)k;
+    run += nk;
+  }
+  if (threadIdx.x == blockDim.x - 1) d.itemoff[n] = run;
 }
 
 // Host driver for steps 1-6 on `stream`.
@@ -370,7 +435,7 @@ int build_clusters(const ClusterLayout &L, const ClusterData<T> &d, void *ws, co
   TFF_LAUNCHED();
   scatter_atoms_kernel<T><<<nb_atoms, 256, 0, s>>>(L.natoms, d);
   TFF_LAUNCHED();
-  const int nb_keys = (int)std::max<int64_t>(1, std::min<int64_t>((std::max(L.nkeys, L.npad - L.natoms) + 127) / 128, sms * 16));
+  const int nb_keys = (int)std::max<int64_t>(1, std::min<int64_t>((L.nkeys + 3) / 4, sms * 32));
   sort_buckets_kernel<T><<<nb_keys, 128, 0, s>>>(x, q, L.nkeys, d);
   TFF_LAUNCHED();
   const int nb_cl = (int)std::max<int64_t>(1, std::min<int64_t>((L.nclusters + 3) / 4, sms * 16));

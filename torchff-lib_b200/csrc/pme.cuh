@@ -92,37 +92,41 @@ struct SortedAtoms {
   }
 };
 
+// Spread: a group of kLanesPerAtom lanes per atom; lane g of the group takes the stencil
+// rows r = g, g + kLanesPerAtom, ... of the 36 (x, y) rows, 6 z points each. Loops run at
+// warp granularity so that every lane of a warp takes the same trip count.
+constexpr int kLanesPerAtom = 8;
+constexpr int kAtomsPerWarp = kWarp / kLanesPerAtom;
+
 template <class T, class Atoms>
 __global__ void __launch_bounds__(kPmeBlock) pme_spread_kernel(Atoms atoms, int64_t nthreads, const T *box, int K,
                                                                typename Acc<T>::S *grid) {
   __shared__ PmeShared sh;
   if (threadIdx.x == 0) load_pme_shared(box, K, sh);
   __syncthreads();
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nthreads; t += stride) {
+  const int g = threadIdx.x % kLanesPerAtom;
+  const int64_t wglob = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  const int64_t nwarps = (int64_t)gridDim.x * blockDim.x / kWarp;
+  for (int64_t wb = wglob * kAtomsPerWarp; wb < nthreads; wb += nwarps * kAtomsPerWarp) {
+    const int64_t t = wb + (threadIdx.x % kWarp) / kLanesPerAtom;
     double rx, ry, rz;
     T q;
-    if (!atoms.get(t, rx, ry, rz, q)) continue;
+    if (t >= nthreads || !atoms.get(t, rx, ry, rz, q)) continue;
     Stencil<T> s;
     make_stencil<T>(rx, ry, rz, sh.recip, K, s);
-    int gx = s.g0[0];
-#pragma unroll 1
-    for (int a = 0; a < 6; ++a) {
-      const T wx = q * s.val[0][a];
-      int gy = s.g0[1];
+    for (int r = g; r < 36; r += kLanesPerAtom) {
+      const int a = r / 6, b = r % 6;
+      int gx = s.g0[0] + a, gy = s.g0[1] + b;
+      gx -= (gx >= K) ? K : 0;
+      gy -= (gy >= K) ? K : 0;
+      const T wxy = q * s.val[0][a] * s.val[1][b];
+      const int64_t row = ((int64_t)gx * K + gy) * K;
+      int gz = s.g0[2];
 #pragma unroll
-      for (int b = 0; b < 6; ++b) {
-        const T wxy = wx * s.val[1][b];
-        const int64_t row = ((int64_t)gx * K + gy) * K;
-        int gz = s.g0[2];
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-          Acc<T>::add(&grid[row + gz], (double)(wxy * s.val[2][c]));
-          gz = (gz + 1 == K) ? 0 : gz + 1;
-        }
-        gy = (gy + 1 == K) ? 0 : gy + 1;
+      for (int c = 0; c < 6; ++c) {
+        Acc<T>::add(&grid[row + gz], (double)(wxy * s.val[2][c]));
+        gz = (gz + 1 == K) ? 0 : gz + 1;
       }
-      gx = (gx + 1 == K) ? 0 : gx + 1;
     }
   }
 }
@@ -178,7 +182,7 @@ __global__ void __launch_bounds__(kPmeBlock) pme_convolve_kernel(typename CplxOf
   grid_sum<kPmeBlock>(0.5 * e, partials, ticket, e_rec, false);
 }
 
-// Gather outputs: plain caller arrays (original order) ...
+// Gather output: caller arrays (caller order), plain stores (one thread per atom).
 template <class T>
 struct PlainGatherOut {
   T *phi;    // dE/dq (N), nullable
@@ -193,20 +197,8 @@ struct PlainGatherOut {
   }
 };
 
-// ... or cluster-sorted accumulators of the fused system (scaled by the Coulomb constant).
-template <class T>
-struct SortedGatherOut {
-  typename Acc<T>::S *gx;  // (npad, 3) sorted slots, dE/dx
-  typename Acc<T>::S *gq;  // (npad) sorted slots, dE/dq
-  double scale;
-  __device__ __forceinline__ void put(int64_t t, double phi_t, double x, double y, double z) const {
-    Acc<T>::add(&gx[3 * t], scale * x);
-    Acc<T>::add(&gx[3 * t + 1], scale * y);
-    Acc<T>::add(&gx[3 * t + 2], scale * z);
-    if (gq) Acc<T>::add(&gq[t], scale * phi_t);
-  }
-};
-
+// Gather: kLanesPerAtom lanes per atom as in the spread, partial sums reduced with
+// shuffles inside the lane group (FP64 accumulation of the 216 products).
 template <class T, class Atoms, class Out>
 __global__ void __launch_bounds__(kPmeBlock) pme_gather_kernel(Atoms atoms, int64_t nthreads, const T *box, int K,
                                                                const T *Phi, double alpha, Out out, double *partials,
@@ -216,50 +208,57 @@ __global__ void __launch_bounds__(kPmeBlock) pme_gather_kernel(Atoms atoms, int6
   if (threadIdx.x == 0) load_pme_shared(box, K, sh);
   __syncthreads();
   const double a_rpi = alpha / 1.7724538509055160273;
+  const int g = threadIdx.x % kLanesPerAtom;
+  const int64_t wglob = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  const int64_t nwarps = (int64_t)gridDim.x * blockDim.x / kWarp;
   double e = 0.0;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nthreads; t += stride) {
-    double rx, ry, rz;
-    T q;
-    if (!atoms.get(t, rx, ry, rz, q)) continue;
-    Stencil<T> s;
-    make_stencil<T>(rx, ry, rz, sh.recip, K, s);
+  for (int64_t wb = wglob * kAtomsPerWarp; wb < nthreads; wb += nwarps * kAtomsPerWarp) {
+    const int64_t t = wb + (threadIdx.x % kWarp) / kLanesPerAtom;
+    double rx = 0.0, ry = 0.0, rz = 0.0;
+    T q = T(0);
+    const bool ok = t < nthreads && atoms.get(t, rx, ry, rz, q);
     double phi = 0.0, du0 = 0.0, du1 = 0.0, du2 = 0.0;
-    int gx = s.g0[0];
-#pragma unroll 1
-    for (int a = 0; a < 6; ++a) {
-      int gy = s.g0[1];
-      double p_a = 0.0, d1_a = 0.0, d2_a = 0.0;
-#pragma unroll
-      for (int b = 0; b < 6; ++b) {
+    Stencil<T> s;
+    if (ok) {
+      make_stencil<T>(rx, ry, rz, sh.recip, K, s);
+      for (int r = g; r < 36; r += kLanesPerAtom) {
+        const int a = r / 6, b = r % 6;
+        int gx = s.g0[0] + a, gy = s.g0[1] + b;
+        gx -= (gx >= K) ? K : 0;
+        gy -= (gy >= K) ? K : 0;
         const int64_t row = ((int64_t)gx * K + gy) * K;
         int gz = s.g0[2];
         T pz = T(0), dz = T(0);
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
-          const T g = Phi[row + gz];
-          pz += g * s.val[2][c];
-          dz += g * s.der[2][c];
+          const T v = Phi[row + gz];
+          pz += v * s.val[2][c];
+          dz += v * s.der[2][c];
           gz = (gz + 1 == K) ? 0 : gz + 1;
         }
-        p_a += (double)(pz * s.val[1][b]);
-        d1_a += (double)(pz * s.der[1][b]);
-        d2_a += (double)(dz * s.val[1][b]);
-        gy = (gy + 1 == K) ? 0 : gy + 1;
+        const double vx = (double)s.val[0][a], vy = (double)s.val[1][b];
+        phi += vx * vy * (double)pz;
+        du0 += (double)s.der[0][a] * vy * (double)pz;
+        du1 += vx * (double)s.der[1][b] * (double)pz;
+        du2 += vx * vy * (double)dz;
       }
-      phi += p_a * (double)s.val[0][a];
-      du0 += p_a * (double)s.der[0][a];
-      du1 += d1_a * (double)s.val[0][a];
-      du2 += d2_a * (double)s.val[0][a];
-      gx = (gx + 1 == K) ? 0 : gx + 1;
     }
-    // u_d = m0 - frac_d + const, so d(stencil u)/dr_c = -recip[d][c]
-    const double qd = (double)q;
-    const double gxv = -qd * (du0 * sh.recip[0] + du1 * sh.recip[3] + du2 * sh.recip[6]);
-    const double gyv = -qd * (du0 * sh.recip[1] + du1 * sh.recip[4] + du2 * sh.recip[7]);
-    const double gzv = -qd * (du0 * sh.recip[2] + du1 * sh.recip[5] + du2 * sh.recip[8]);
-    out.put(t, phi - 2.0 * a_rpi * qd, gxv, gyv, gzv);
-    e -= a_rpi * qd * qd;
+#pragma unroll
+    for (int o = kLanesPerAtom / 2; o > 0; o >>= 1) {
+      phi += __shfl_xor_sync(kFull, phi, o);
+      du0 += __shfl_xor_sync(kFull, du0, o);
+      du1 += __shfl_xor_sync(kFull, du1, o);
+      du2 += __shfl_xor_sync(kFull, du2, o);
+    }
+    if (ok && g == 0) {
+      // u_d = m0 - frac_d + const, so d(stencil u)/dr_c = -recip[d][c]
+      const double qd = (double)q;
+      const double gxv = -qd * (du0 * sh.recip[0] + du1 * sh.recip[3] + du2 * sh.recip[6]);
+      const double gyv = -qd * (du0 * sh.recip[1] + du1 * sh.recip[4] + du2 * sh.recip[7]);
+      const double gzv = -qd * (du0 * sh.recip[2] + du1 * sh.recip[5] + du2 * sh.recip[8]);
+      out.put(t, phi - 2.0 * a_rpi * qd, gxv, gyv, gzv);
+      e -= a_rpi * qd * qd;
+    }
   }
   const bool last = grid_sum<kPmeBlock>(e, partials, ticket, e_self, false);
   if (last && threadIdx.x == 0 && energy_out) energy_out[0] = (T)(e_scale * (*e_rec + *e_self));
@@ -321,7 +320,8 @@ int pme_grid_phase(const PmePlanImpl &p, const PmeLayout &L, char *ws, Atoms ato
   const int sms = sm_count();
   S *grid = reinterpret_cast<S *>(ws + L.fix);
   if (nthreads > 0) {
-    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((nthreads + kPmeBlock - 1) / kPmeBlock, sms * 8));
+    const int64_t lanes = nthreads * kLanesPerAtom;
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((lanes + kPmeBlock - 1) / kPmeBlock, sms * 8));
     pme_spread_kernel<T, Atoms><<<nb, kPmeBlock, 0, s>>>(atoms, nthreads, box, K, grid);
     TFF_LAUNCHED();
   }
@@ -368,7 +368,8 @@ int pme_gather_phase(const PmePlanImpl &p, const PmeLayout &L, char *ws, Atoms a
   double *partials = reinterpret_cast<double *>(ws + L.partials);
   unsigned *tickets = reinterpret_cast<unsigned *>(ws + L.tickets);
   double *energies = reinterpret_cast<double *>(ws + L.energies);
-  const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((nthreads + kPmeBlock - 1) / kPmeBlock, sm_count() * 8));
+  const int64_t lanes = nthreads * kLanesPerAtom;
+  const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((lanes + kPmeBlock - 1) / kPmeBlock, sm_count() * 8));
   pme_gather_kernel<T, Atoms, Out><<<nb, kPmeBlock, 0, s>>>(atoms, nthreads, box, p.K, phi_grid, alpha, out,
                                                             partials, tickets + 1, energies + 1, energies, e_scale,
                                                             energy_out);

@@ -21,8 +21,9 @@ LIB_NAME = "libtffb200.so"
 SOURCES = ["tff_common.cu", "pairs.cu", "nblist.cu", "pme.cu", "fused.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# -ftz=true: FP32 subnormals flush to zero (none arise on this path); FP64 is unaffected
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
-              "-Xptxas", "-warn-spills"]
+              "-ftz=true", "-Xptxas", "-warn-spills"]
 
 
 def nvcc() -> str:

@@ -135,11 +135,12 @@ class FixedChargeSystem:
 class StageTimer:
     """CUDA events at the stage boundaries of a fused evaluation.
 
-    Event k: 0 start, 1 cluster build, 2 real-space tile kernel, 3 PME grid phase
-    (spread, FFTs, influence function), 4 PME gather, 5 finalize.
+    Event k: 0 start, 1 cluster build done, 2 real-space tile kernel done (caller stream);
+    3 PME grid phase done (spread, FFTs, influence function), 4 PME gather done (PME
+    stream, forked at event 0); 5 finalize done (after both branches joined).
     """
 
-    STAGES = ("cluster_build", "tile_kernel", "pme_grid", "pme_gather", "finalize")
+    STAGES = ("cluster_build", "tile_kernel", "pme_grid", "pme_gather", "finalize", "total")
 
     def __init__(self):
         h = ctypes.c_void_p()
@@ -152,7 +153,11 @@ class StageTimer:
         return float(v.value)
 
     def stages_ms(self) -> dict:
-        return {name: self.elapsed_ms(k, k + 1) for k, name in enumerate(self.STAGES)}
+        out = {"cluster_build": self.elapsed_ms(0, 1), "tile_kernel": self.elapsed_ms(1, 2),
+               "pme_grid": self.elapsed_ms(0, 3), "pme_gather": self.elapsed_ms(3, 4)}
+        out["finalize"] = min(self.elapsed_ms(2, 5), self.elapsed_ms(4, 5))
+        out["total"] = self.elapsed_ms(0, 5)
+        return out
 
     def __del__(self):
         h = getattr(self, "handle", None)
