@@ -70,9 +70,10 @@ int tff_nblist_nsquared(int dtype, int64_t natoms, const void *coords, const voi
 
 /* Replaces torch.ops.torchff.build_neighbor_list_cell_list / _out
  * (csrc/nblist/nblist_interface.cpp:7-8, csrc/nblist/nblist_clist_cuda.cu:367-525).
- * Same output contract as tff_nblist_nsquared; requires an orthorhombic `box`. Atoms are
- * binned on a Morton-ordered cell grid, grouped in 32-atom clusters and cluster pairs are
- * screened by bounding boxes before a 32x32 warp tile test.
+ * Same output contract as tff_nblist_nsquared; needs a periodic `box` (any shape). Atoms
+ * are binned on a Hilbert-ordered cell grid, grouped in 32-atom clusters and cluster pairs
+ * are screened by bounding boxes (exact for orthorhombic boxes, conservative otherwise)
+ * before a 32x32 warp tile test.
  * max_cluster_neighbors: capacity of each cluster's neighbour-cluster list (0 = default). */
 size_t tff_nblist_cell_list_workspace_bytes(int dtype, int64_t natoms, int max_cluster_neighbors);
 int tff_nblist_cell_list(int dtype, int64_t natoms, const void *coords, const void *box,

@@ -175,3 +175,32 @@ def test_fused_matches_operator_composition(ref216):
     e.backward()
     assert rel(e.item(), ref["total"]) < 1e-10
     assert rel_max(x.grad, ref["grad_coords"]) < 1e-8
+
+
+def test_large_box_matches_independent_composition():
+    """12,000 waters (36,000 atoms): the cell grid is rounded to 16^3 (power-of-two branch).
+    Fused FP64 vs the O(N^2) pair list + pair ops + PME op composition, and mixed vs FP64."""
+    from torchff_b200 import PME, MultipolarInteraction, NeighborList, Vdw
+    from torchff_b200.system import FixedChargeSystem
+    from torchff_b200.water import make_water_box
+
+    wb = make_water_box(12000, 4.482 * (4.0 ** (1.0 / 3.0)), 23, cutoff=1.0, grid=72, seed=3)
+    s64 = FixedChargeSystem.from_water_box(wb, dtype=torch.float64)
+    out = s64.evaluate(t(wb.coords), t(wb.box))
+    assert s64.status() == 0
+    x, b, q = t(wb.coords, grad=True), t(wb.box), t(wb.charges)
+    nbl = NeighborList(wb.natoms, exclusions=torch.tensor(wb.nblist_exclusions), algorithm="nsquared").cuda()
+    pairs, npairs = nbl(x.detach(), b, wb.cutoff, 8_000_000, padding=True)
+    assert int(npairs.item()) <= 8_000_000
+    e = (Vdw("LennardJones", use_customized_ops=True, use_type_pairs=True)(
+            x, pairs, b, t(wb.sigma_table), t(wb.epsilon_table), wb.cutoff, atom_types=t(wb.atom_types, torch.int64))
+         + MultipolarInteraction(0, wb.cutoff, wb.alpha, 138.935456)(
+            x, b, pairs, q, pairs_excl=t(wb.coulomb_exclusions, torch.int64))
+         + PME(wb.alpha, wb.grid, 0, use_customized_ops=True).cuda()(x, b, q) * 138.935456)
+    e.backward()
+    assert rel(out["energy"].item(), e.item()) < 1e-10
+    assert rel_max(out["forces"], -x.grad) < 1e-8
+    s32 = FixedChargeSystem.from_water_box(wb, dtype=torch.float32)
+    o32 = s32.evaluate(t(wb.coords, torch.float32), t(wb.box, torch.float32))
+    assert s32.status() == 0
+    assert rel_rms(o32["forces"], out["forces"]) < 1e-5

@@ -1,7 +1,7 @@
 // Cluster build shared by the cell-list neighbour list and the fused real-space kernel.
 //
 // 1. cell_keys:      fractional coordinates wrapped to [0,1), cell on an nc^3 grid
-//                    (about 8 atoms per cell), Morton key, per-key histogram.
+//                    (about 8 atoms per cell), Hilbert-curve key, per-key histogram.
 // 2. scan_keys:      exclusive scan of the histogram (one block, segmented).
 // 3. scatter_atoms:  atoms into key buckets (slot order inside a bucket is arbitrary).
 // 4. sort_buckets:   one warp per bucket ranks its atoms by index -> deterministic order; writes the
@@ -12,8 +12,8 @@
 //                    those whose boxes can hold a pair within the cutoff (order of the
 //                    list is deterministic). `half` keeps only J <= I.
 //
-// The Morton order of ~8-atom cells makes 32 consecutive atoms a compact blob (a 2x2x1
-// block of cells), which is what the 32x32 warp tiles need.
+// Along the Hilbert curve of ~8-atom cells, 32 consecutive atoms form a compact blob of
+// about 4 face-connected cells, which is what the 32x32 warp tiles need.
 #pragma once
 
 #include <climits>
@@ -45,9 +45,13 @@ struct ClusterLayout {
 inline ClusterLayout cluster_layout(int dtype, int64_t natoms, int cap) {
   ClusterLayout L;
   L.natoms = natoms;
-  // ~8 atoms per cell: with Morton order, runs of 32 atoms form the most compact clusters
-  // (fewest cluster pairs within the cutoff) among 2..32 atoms per cell on water boxes
-  int nc = (int)floor(cbrt((double)natoms / 8.0));
+  // ~8 atoms per cell: runs of 32 atoms along the curve form the most compact clusters
+  // (fewest cluster pairs within the cutoff) among 2..32 atoms per cell on water boxes.
+  // From 16 cells per side up, the side is rounded to a power of two: on a grid that only
+  // partly fills its 2^b key space the curve leaves and re-enters the grid, and a 32-atom
+  // run across such a jump is not compact (small boxes bound the damage).
+  const double g = cbrt((double)natoms / 8.0);
+  int nc = g >= 16.0 ? (1 << (int)lround(log2(g))) : (int)floor(g);
   nc = std::max(1, std::min(nc, 128));
   int bits = 0;
   while ((1 << bits) < nc) ++bits;
@@ -126,13 +130,40 @@ inline ClusterData<T> cluster_data(const ClusterLayout &L, void *ws) {
   return d;
 }
 
-__device__ __forceinline__ unsigned morton_spread(unsigned v) {
-  v &= 0x3ff;
-  v = (v | (v << 16)) & 0x030000FF;
-  v = (v | (v << 8)) & 0x0300F00F;
-  v = (v | (v << 4)) & 0x030C30C3;
-  v = (v | (v << 2)) & 0x09249249;
-  return v;
+// Index of cell (x0, x1, x2) along the 3-D Hilbert curve of a 2^b grid, from J. Skilling,
+// "Programming the Hilbert curve", AIP Conf. Proc. 707, 381 (2004): the axes are turned
+// into the transposed Hilbert index (inverse undo, then Gray encoding), whose bits are
+// interleaved with x0 most significant. Unlike the Morton (Z-order) curve, consecutive
+// Hilbert cells are always face neighbours, so a run of 32 atoms never jumps across the box.
+__device__ __forceinline__ unsigned hilbert_key(unsigned x0, unsigned x1, unsigned x2, int b) {
+  if (b <= 0) return 0u;
+  unsigned X[3] = {x0, x1, x2};
+  const unsigned M = 1u << (b - 1);
+  for (unsigned Q = M; Q > 1u; Q >>= 1) {
+    const unsigned P = Q - 1u;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        const unsigned t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  X[1] ^= X[0];
+  X[2] ^= X[1];
+  unsigned t = 0u;
+  for (unsigned Q = M; Q > 1u; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1u;
+  X[0] ^= t;
+  X[1] ^= t;
+  X[2] ^= t;
+  unsigned key = 0u;
+  for (int bit = b - 1; bit >= 0; --bit)
+    key = (key << 3) | (((X[0] >> bit) & 1u) << 2) | (((X[1] >> bit) & 1u) << 1) | ((X[2] >> bit) & 1u);
+  return key;
 }
 
 // Box facts used by the cluster search: inverse, orthorhombic flag, perpendicular widths.
@@ -174,7 +205,7 @@ __global__ void cell_keys_kernel(const T *x, int64_t n, ClusterData<T> d) {
     unsigned cell[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) cell[c] = min((unsigned)(f[c] * d.nc), (unsigned)(d.nc - 1));
-    unsigned key = (morton_spread(cell[0]) << 2) | (morton_spread(cell[1]) << 1) | morton_spread(cell[2]);
+    const unsigned key = hilbert_key(cell[0], cell[1], cell[2], d.bits);
     d.keys[i] = key;
     atomicAdd(&d.hist[key], 1u);
   }

@@ -501,6 +501,8 @@ struct tff_system_s {
   void *dev_x = nullptr;       // coords/box in system dtype for *_host
   double *dev_f = nullptr;     // forces64 for *_host
   double *dev_e = nullptr;
+  cudaGraphExec_t host_graph = nullptr;  // device part of tff_system_eval_host, captured once
+  cudaStream_t capture_stream = nullptr;
 };
 
 namespace tff {
@@ -615,6 +617,8 @@ void free_system(tff_system sys) {
   if (sys->pme_stream) cudaStreamDestroy(sys->pme_stream);
   if (sys->fork_ev) cudaEventDestroy(sys->fork_ev);
   if (sys->join_ev) cudaEventDestroy(sys->join_ev);
+  if (sys->host_graph) cudaGraphExecDestroy(sys->host_graph);
+  if (sys->capture_stream) cudaStreamDestroy(sys->capture_stream);
   void *ptrs[] = {sys->cl_ws, sys->pme_ws, sys->acc, sys->lj, sys->exslot, sys->pme_grad, sys->pme_phi,
                   sys->q, sys->sigma, sys->eps, sys->excl, sys->moduli, sys->scratch, sys->host_x,
                   sys->dev_x, sys->dev_f, sys->dev_e};
@@ -661,7 +665,7 @@ int tff_system_create(const tff_system_desc *desc, const double *charges, const 
   sys->desc = *desc;
   const int64_t ncl = (n + kWarp - 1) / kWarp;
   sys->cap = desc->max_cluster_neighbors > 0 ? desc->max_cluster_neighbors
-                                             : (int)std::max<int64_t>(1, std::min<int64_t>(ncl, 512));
+                                             : (int)std::max<int64_t>(1, std::min<int64_t>(ncl, 1024));
   sys->cl = cluster_layout(desc->dtype, n, sys->cap);
   const size_t ts = desc->dtype == TFF_F64 ? 8 : 4;
 #define TFF_ALLOC(ptr, bytes)                                              \
@@ -773,22 +777,42 @@ int tff_system_eval_host(tff_system sys, const double *coords, const double *box
   TFF_ARG(n == 0 || (coords != nullptr && forces != nullptr), "coords/forces is NULL");
   cudaStream_t s = (cudaStream_t)stream;
   double *stage = static_cast<double *>(sys->host_x);
+  // The device part (FP64 -> system dtype cast + evaluation into internal buffers) only
+  // touches the system's own buffers, so it is captured into a CUDA graph on the first
+  // call (on an internal stream) and replayed on `stream` afterwards.
+  if (sys->host_graph == nullptr) {
+    if (sys->capture_stream == nullptr)
+      TFF_CUDA(cudaStreamCreateWithFlags(&sys->capture_stream, cudaStreamNonBlocking));
+    cudaStream_t cs = sys->capture_stream;
+    TFF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    int st;
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((3 * n + 255) / 256, sm_count() * 8));
+    if (sys->desc.dtype == TFF_F32) {
+      float *x = static_cast<float *>(sys->dev_x);
+      cast_inputs_kernel<float><<<nb, 256, 0, cs>>>(stage, stage + 3 * n, x, x + 3 * n, 3 * n);
+      st = system_eval_impl<float>(sys, x, x + 3 * n, sys->dev_e, nullptr, sys->dev_f, nullptr, nullptr, cs);
+    } else {
+      double *x = static_cast<double *>(sys->dev_x);
+      cast_inputs_kernel<double><<<nb, 256, 0, cs>>>(stage, stage + 3 * n, x, x + 3 * n, 3 * n);
+      st = system_eval_impl<double>(sys, x, x + 3 * n, sys->dev_e, nullptr, sys->dev_f, nullptr, nullptr, cs);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(cs, &graph);
+    if (st != TFF_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+    const cudaError_t ie = cudaGraphInstantiate(&sys->host_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      sys->host_graph = nullptr;
+      return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+    }
+  }
   if (n > 0) TFF_CUDA(cudaMemcpyAsync(stage, coords, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
   TFF_CUDA(cudaMemcpyAsync(stage + 3 * n, box, 9 * sizeof(double), cudaMemcpyHostToDevice, s));
-  int st;
-  const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((3 * n + 255) / 256, sm_count() * 8));
-  if (sys->desc.dtype == TFF_F32) {
-    float *x = static_cast<float *>(sys->dev_x);
-    cast_inputs_kernel<float><<<nb, 256, 0, s>>>(stage, stage + 3 * n, x, x + 3 * n, 3 * n);
-    TFF_LAUNCHED();
-    st = system_eval_impl<float>(sys, x, x + 3 * n, sys->dev_e, nullptr, sys->dev_f, nullptr, nullptr, s);
-  } else {
-    double *x = static_cast<double *>(sys->dev_x);
-    cast_inputs_kernel<double><<<nb, 256, 0, s>>>(stage, stage + 3 * n, x, x + 3 * n, 3 * n);
-    TFF_LAUNCHED();
-    st = system_eval_impl<double>(sys, x, x + 3 * n, sys->dev_e, nullptr, sys->dev_f, nullptr, nullptr, s);
-  }
-  if (st != TFF_OK) return st;
+  TFF_CUDA(cudaGraphLaunch(sys->host_graph, s));
   if (n > 0) TFF_CUDA(cudaMemcpyAsync(forces, sys->dev_f, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   TFF_CUDA(cudaMemcpyAsync(energy, sys->dev_e, sizeof(double), cudaMemcpyDeviceToHost, s));
   TFF_CUDA(cudaStreamSynchronize(s));

@@ -229,7 +229,7 @@ __global__ void cluster_overflow_kernel(const unsigned *status, int32_t *npairs)
 
 int default_cluster_cap(int64_t nclusters, int requested) {
   if (requested > 0) return requested;
-  return (int)std::max<int64_t>(1, std::min<int64_t>(nclusters, 512));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(nclusters, 1024));
 }
 
 template <class T>
