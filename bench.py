@@ -17,6 +17,7 @@ cores, rank 0 only.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import math
 import os
@@ -64,7 +65,9 @@ def water_box(name: str, seed: int):
 # ---------------------------------------------------------------------------------------
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi clock/throttle samples every 50 ms; only samples whose own timestamp lies
+    inside [begin(), end()] count, so the sampler's start-up time is not mistaken for load."""
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -72,15 +75,22 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.t_begin = self.t_end = None
 
-    def start(self):
+    def start(self, settle_s: float = 1.5):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(settle_s)
         except OSError:
             self.proc = None
-        self.t0 = time.time()
+
+    def begin(self):
+        self.t_begin = datetime.datetime.now()
+
+    def end(self):
+        self.t_end = datetime.datetime.now()
 
     def stop(self):
         if self.proc is None:
@@ -98,14 +108,17 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f")
+                if self.t_begin is not None and not (self.t_begin <= ts <= self.t_end):
+                    continue
+                sm.append(float(f[2]))
+                smax = float(f[3])
             except ValueError:
                 continue
-            for name, v in zip(names, f[5:9]):
+            for name, v in zip(names, f[6:10]):
                 if v.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
@@ -180,8 +193,6 @@ def run_ours(args):
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     if world > 1:
-        import datetime
-
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
 
     import torchff_b200  # noqa: F401
@@ -222,6 +233,7 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(device)
+    clocks.begin()
     step_ms, tile_ms, stage_acc = [], [], {k: 0.0 for k in StageTimer.STAGES}
     for i in range(args.steps):
         flush.fill_(i & 0xff)
@@ -235,6 +247,7 @@ def run_ours(args):
         for k, v in st.items():
             stage_acc[k] += v
     torch.cuda.synchronize(device)
+    clocks.end()
     if world > 1:
         dist.barrier()
     clocks.stop()

@@ -25,6 +25,9 @@ namespace tff {
 // Neighbour clusters per tile-kernel work item (a work item is one cluster I and every
 // (ncount/kItemTiles)-th cluster of its list).
 constexpr int kItemTiles = 8;
+// Consecutive clusters per super-cluster: the neighbour search screens a super-cluster's
+// union box first and tests its members only when that box is within the cutoff.
+constexpr int kSuper = 32;
 
 template <class T> struct V4;
 template <> struct V4<float> { using type = float4; };
@@ -36,9 +39,9 @@ __device__ __forceinline__ float4 make_v4(float x, float y, float z, float w) { 
 
 struct ClusterLayout {
   int nc = 1, bits = 0;
-  int64_t nkeys = 1, natoms = 0, nclusters = 0, npad = 0;
+  int64_t nkeys = 1, natoms = 0, nclusters = 0, npad = 0, nsuper = 0;
   int cap = 0;
-  size_t keys, hist, fill, status, tmp, sidx, inv, pos, frac, bc, bh, nbr, ncount, itemoff, items, boxinfo;
+  size_t keys, hist, fill, status, tmp, sidx, inv, pos, frac, bc, bh, sbc, sbh, nbr, ncount, itemoff, items, boxinfo;
   size_t zero_off, zero_bytes, bytes;
 };
 
@@ -60,6 +63,7 @@ inline ClusterLayout cluster_layout(int dtype, int64_t natoms, int cap) {
   L.nkeys = (int64_t)1 << (3 * bits);
   L.nclusters = (natoms + kWarp - 1) / kWarp;
   L.npad = L.nclusters * kWarp;
+  L.nsuper = (L.nclusters + kSuper - 1) / kSuper;
   L.cap = cap;
   const size_t tsz = dtype == TFF_F64 ? 8 : 4;
   Carver c(nullptr);
@@ -77,6 +81,8 @@ inline ClusterLayout cluster_layout(int dtype, int64_t natoms, int cap) {
   L.frac = (c.off + 255) & ~size_t(255); c.take<char>(L.npad * 4 * tsz);
   L.bc = (c.off + 255) & ~size_t(255); c.take<char>(L.nclusters * 4 * tsz);
   L.bh = (c.off + 255) & ~size_t(255); c.take<char>(L.nclusters * 4 * tsz);
+  L.sbc = (c.off + 255) & ~size_t(255); c.take<char>(L.nsuper * 4 * tsz);
+  L.sbh = (c.off + 255) & ~size_t(255); c.take<char>(L.nsuper * 4 * tsz);
   L.nbr = (c.off + 255) & ~size_t(255); c.take<int>((size_t)L.nclusters * cap);
   L.ncount = (c.off + 255) & ~size_t(255); c.take<int>(L.nclusters);
   L.itemoff = (c.off + 255) & ~size_t(255); c.take<int>(L.nclusters + 1);
@@ -95,9 +101,10 @@ struct ClusterData {
   int *itemoff;  // work items of the tile kernel: prefix sums of ceil(ncount / kItemTiles)
   int *items;    // owning cluster of each work item
   V *pos, *frac, *bc, *bh;
+  V *sbc, *sbh;     // union boxes of kSuper consecutive clusters (fractional centre, half extent)
   double *boxinfo;  // [0..8] box, [9..17] inv, [18] ortho flag, [19..21] perpendicular widths
   int nc, bits, cap;
-  int64_t natoms, nclusters, npad;
+  int64_t natoms, nclusters, npad, nsuper;
 };
 
 template <class T>
@@ -120,6 +127,8 @@ inline ClusterData<T> cluster_data(const ClusterLayout &L, void *ws) {
   d.frac = reinterpret_cast<V *>(b + L.frac);
   d.bc = reinterpret_cast<V *>(b + L.bc);
   d.bh = reinterpret_cast<V *>(b + L.bh);
+  d.sbc = reinterpret_cast<V *>(b + L.sbc);
+  d.sbh = reinterpret_cast<V *>(b + L.sbh);
   d.boxinfo = reinterpret_cast<double *>(b + L.boxinfo);
   d.nc = L.nc;
   d.bits = L.bits;
@@ -127,6 +136,7 @@ inline ClusterData<T> cluster_data(const ClusterLayout &L, void *ws) {
   d.natoms = L.natoms;
   d.nclusters = L.nclusters;
   d.npad = L.npad;
+  d.nsuper = L.nsuper;
   return d;
 }
 
@@ -313,49 +323,87 @@ __global__ void sort_buckets_kernel(const T *x, const T *q, int64_t nkeys, Clust
 // the first atom's image so that a cluster straddling the periodic boundary stays compact,
 // and the cluster's positions are rewritten as that same contiguous image (anchor +
 // nearest-image offset), so that one periodic shift serves a whole cluster pair.
+// A block of kSuper warps covers one super-cluster and, once its member boxes are known,
+// takes their union around the first member's centre (members shifted to their nearest
+// image of it) and widens it by 1e-5 to cover the rounding of centres to T.
 template <class T>
-__global__ void cluster_bounds_kernel(ClusterData<T> d) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+__global__ void __launch_bounds__(kWarp * kSuper) cluster_bounds_kernel(ClusterData<T> d) {
+  __shared__ double s_box[kSuper][6];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const double *m = d.boxinfo;
-  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < d.nclusters; c += nw) {
-    const int64_t s = c * kWarp + lane;
-    const bool valid = d.sidx[s] >= 0;
-    auto f = d.frac[s];
-    T fx = f.x, fy = f.y, fz = f.z;
-    const T ax = __shfl_sync(kFull, fx, 0), ay = __shfl_sync(kFull, fy, 0), az = __shfl_sync(kFull, fz, 0);
-    fx -= ax; fy -= ay; fz -= az;
-    fx -= floor(fx + T(0.5)); fy -= floor(fy + T(0.5)); fz -= floor(fz + T(0.5));
-    if (valid) {
-      const double ux = (double)ax + (double)fx, uy = (double)ay + (double)fy, uz = (double)az + (double)fz;
-      auto p = d.pos[s];
-      p.x = (T)(ux * m[0] + uy * m[3] + uz * m[6]);
-      p.y = (T)(ux * m[1] + uy * m[4] + uz * m[7]);
-      p.z = (T)(ux * m[2] + uy * m[5] + uz * m[8]);
-      d.pos[s] = p;
-    }
-    T lo[3] = {valid ? fx : T(1e30), valid ? fy : T(1e30), valid ? fz : T(1e30)};
-    T hi[3] = {valid ? fx : T(-1e30), valid ? fy : T(-1e30), valid ? fz : T(-1e30)};
+  for (int64_t S = blockIdx.x; S < d.nsuper; S += gridDim.x) {
+    const int64_t c = S * kSuper + w;
+    if (c < d.nclusters) {
+      const int64_t s = c * kWarp + lane;
+      const bool valid = d.sidx[s] >= 0;
+      auto f = d.frac[s];
+      T fx = f.x, fy = f.y, fz = f.z;
+      const T ax = __shfl_sync(kFull, fx, 0), ay = __shfl_sync(kFull, fy, 0), az = __shfl_sync(kFull, fz, 0);
+      fx -= ax; fy -= ay; fz -= az;
+      fx -= floor(fx + T(0.5)); fy -= floor(fy + T(0.5)); fz -= floor(fz + T(0.5));
+      if (valid) {
+        const double ux = (double)ax + (double)fx, uy = (double)ay + (double)fy, uz = (double)az + (double)fz;
+        auto p = d.pos[s];
+        p.x = (T)(ux * m[0] + uy * m[3] + uz * m[6]);
+        p.y = (T)(ux * m[1] + uy * m[4] + uz * m[7]);
+        p.z = (T)(ux * m[2] + uy * m[5] + uz * m[8]);
+        d.pos[s] = p;
+      }
+      T lo[3] = {valid ? fx : T(1e30), valid ? fy : T(1e30), valid ? fz : T(1e30)};
+      T hi[3] = {valid ? fx : T(-1e30), valid ? fy : T(-1e30), valid ? fz : T(-1e30)};
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+      for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        lo[k] = min(lo[k], __shfl_xor_sync(kFull, lo[k], o));
-        hi[k] = max(hi[k], __shfl_xor_sync(kFull, hi[k], o));
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = min(lo[k], __shfl_xor_sync(kFull, lo[k], o));
+          hi[k] = max(hi[k], __shfl_xor_sync(kFull, hi[k], o));
+        }
+      }
+      if (lane == 0) {
+        const auto cc = make_v4(ax + T(0.5) * (lo[0] + hi[0]), ay + T(0.5) * (lo[1] + hi[1]),
+                                az + T(0.5) * (lo[2] + hi[2]), T(0));
+        const auto hh = make_v4(T(0.5) * (hi[0] - lo[0]), T(0.5) * (hi[1] - lo[1]), T(0.5) * (hi[2] - lo[2]), T(0));
+        d.bc[c] = cc;
+        d.bh[c] = hh;
+        s_box[w][0] = cc.x; s_box[w][1] = cc.y; s_box[w][2] = cc.z;
+        s_box[w][3] = hh.x; s_box[w][4] = hh.y; s_box[w][5] = hh.z;
       }
     }
-    if (lane == 0) {
-      d.bc[c] = make_v4(ax + T(0.5) * (lo[0] + hi[0]), ay + T(0.5) * (lo[1] + hi[1]),
-                        az + T(0.5) * (lo[2] + hi[2]), T(0));
-      d.bh[c] = make_v4(T(0.5) * (hi[0] - lo[0]), T(0.5) * (hi[1] - lo[1]), T(0.5) * (hi[2] - lo[2]), T(0));
+    __syncthreads();
+    if (w == 0) {
+      const bool v = S * kSuper + lane < d.nclusters;
+      double lo[3], hi[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double ref = s_box[0][k];
+        double u = v ? s_box[lane][k] - ref : 0.0;
+        u -= floor(u + 0.5);
+        lo[k] = v ? ref + u - s_box[lane][3 + k] : 1e30;
+        hi[k] = v ? ref + u + s_box[lane][3 + k] : -1e30;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = fmin(lo[k], __shfl_xor_sync(kFull, lo[k], o));
+          hi[k] = fmax(hi[k], __shfl_xor_sync(kFull, hi[k], o));
+        }
+      }
+      if (lane == 0) {
+        d.sbc[S] = make_v4((T)(0.5 * (lo[0] + hi[0])), (T)(0.5 * (lo[1] + hi[1])), (T)(0.5 * (lo[2] + hi[2])), T(0));
+        d.sbh[S] = make_v4((T)(0.5 * (hi[0] - lo[0]) + 1e-5), (T)(0.5 * (hi[1] - lo[1]) + 1e-5),
+                           (T)(0.5 * (hi[2] - lo[2]) + 1e-5), T(0));
+      }
     }
+    __syncthreads();
   }
 }
 
-// Whether clusters I and J can hold a pair within rc. Fractional per-dimension gaps use
-// the nearest periodic image of the centres (per dimension, the minimum over all images);
-// orthorhombic boxes test sum_d (gap_d L_d)^2 <= rc^2 (exact for boxes), other boxes the
-// conservative max_d gap_d w_d <= rc with w_d the perpendicular widths.
+// Conservative cluster-pair test on fractional boxes: per axis, the gap between the two
+// intervals on the periodic unit circle (nearest image of the centres), converted to a
+// distance with the box (exact for orthorhombic, perpendicular widths otherwise). The gap
+// only shrinks when one box grows, so a super-cluster's union box that fails the test
+// proves that every member fails it too.
 template <class T>
 __device__ __forceinline__ bool clusters_may_interact(const typename V4<T>::type &ci, const typename V4<T>::type &hi,
                                                       const typename V4<T>::type &cj, const typename V4<T>::type &hj,
@@ -386,16 +434,26 @@ __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) 
     const auto hi = d.bh[I];
     int count = 0;
     const int64_t jend = half ? (I + 1) : d.nclusters;
-    for (int64_t base = 0; base < jend; base += kWarp) {
-      const int64_t J = base + lane;
-      bool ok = false;
-      if (J < jend) ok = clusters_may_interact<T>(ci, hi, d.bc[J], d.bh[J], d.boxinfo, rc);
-      const unsigned m = __ballot_sync(kFull, ok);
-      if (ok) {
-        const int r = count + __popc(m & ((1u << lane) - 1u));
-        if (r < d.cap) d.nbr[I * d.cap + r] = (int)J;
+    const int64_t send = (jend + kSuper - 1) / kSuper;
+    // Lanes screen 32 super-clusters at a time; the members of each survivor (one per lane,
+    // kSuper == kWarp) are then tested in ascending order, so the list is sorted by J.
+    for (int64_t sb = 0; sb < send; sb += kWarp) {
+      const int64_t S = sb + lane;
+      const bool sok = S < send && clusters_may_interact<T>(ci, hi, d.sbc[S], d.sbh[S], d.boxinfo, rc);
+      unsigned sm = __ballot_sync(kFull, sok);
+      while (sm) {
+        const int k = __ffs(sm) - 1;
+        sm &= sm - 1u;
+        const int64_t J = (sb + k) * kSuper + lane;
+        bool ok = false;
+        if (J < jend) ok = clusters_may_interact<T>(ci, hi, d.bc[J], d.bh[J], d.boxinfo, rc);
+        const unsigned mm = __ballot_sync(kFull, ok);
+        if (ok) {
+          const int r = count + __popc(mm & ((1u << lane) - 1u));
+          if (r < d.cap) d.nbr[I * d.cap + r] = (int)J;
+        }
+        count += __popc(mm);
       }
-      count += __popc(m);
     }
     if (lane == 0) {
       d.ncount[I] = min(count, d.cap);
@@ -470,7 +528,8 @@ int build_clusters(const ClusterLayout &L, const ClusterData<T> &d, void *ws, co
   sort_buckets_kernel<T><<<nb_keys, 128, 0, s>>>(x, q, L.nkeys, d);
   TFF_LAUNCHED();
   const int nb_cl = (int)std::max<int64_t>(1, std::min<int64_t>((L.nclusters + 3) / 4, sms * 16));
-  cluster_bounds_kernel<T><<<nb_cl, 128, 0, s>>>(d);
+  const int nb_super = (int)std::max<int64_t>(1, std::min<int64_t>(L.nsuper, sms * 2));
+  cluster_bounds_kernel<T><<<nb_super, kWarp * kSuper, 0, s>>>(d);
   TFF_LAUNCHED();
   cluster_neighbors_kernel<T><<<nb_cl, 128, 0, s>>>(d, rc, half);
   TFF_LAUNCHED();
