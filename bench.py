@@ -38,6 +38,8 @@ WORKLOAD_TEXT = {
     "water216": "216 rigid TIP3P waters (648 atoms), cubic L=1.8662 nm, rc=0.9 nm, Ewald alpha 2.920 nm^-1, "
                 "PME 20^3 order 6",
     "water100k": "100,000 rigid TIP3P waters (300,000 atoms), cubic L=14.42 nm, rc=1.0 nm, PME 144^3 order 6",
+    "serving": "4096 requests, each a rigid TIP3P box of log-uniform [64, 4000] waters at 33.4 waters/nm^3, "
+               "rc=0.9 nm, PME grid K=ceil(L/0.1 nm) order 6, mixed precision",
 }
 
 
@@ -51,6 +53,9 @@ def parse():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving section of the water3000 line")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 timing of the water3000 line")
+    ap.add_argument("--serving-requests", type=int, default=4096)
     return ap.parse_args()
 
 
@@ -180,6 +185,154 @@ def cpu_baseline_sample(wb, evals: int = 2) -> dict:
                       f"pair terms, PME with analytic forces), one thread"}
 
 
+def time_graph_evals(wb, dtype, device, steps: int, warmup: int) -> dict:
+    """evals/s of one system by CUDA-graph replays with an L2 flush in between."""
+    import torch
+
+    from torchff_b200.system import FixedChargeSystem
+
+    system = FixedChargeSystem.from_water_box(wb, dtype=dtype, device=device)
+    x = torch.tensor(wb.coords, dtype=dtype, device=device)
+    b = torch.tensor(wb.box, dtype=dtype, device=device)
+    energy = torch.empty(1, dtype=torch.float64, device=device)
+    forces = torch.empty_like(x)
+    side = torch.cuda.Stream(device)
+    side.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            system.evaluate_into(x, b, energy, forces)
+    torch.cuda.current_stream(device).wait_stream(side)
+    torch.cuda.synchronize(device)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        system.evaluate_into(x, b, energy, forces)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i in range(warmup):
+        flush.fill_(i & 0xff)
+        graph.replay()
+    total = 0.0
+    for i in range(steps):
+        flush.fill_(i & 0xff)
+        start.record()
+        graph.replay()
+        end.record()
+        end.synchronize()
+        total += start.elapsed_time(end)
+    del graph
+    return {"value": round(steps / (total / 1e3), 2), "unit": "evals/s", "ms_per_step": round(total / steps, 5),
+            "steps": steps, "warmup": warmup}
+
+
+def run_serving(device, n_requests: int = 4096, seed: int = 0) -> dict:
+    """Continuous-batching server on the serving workload: throughput at saturation, p50/p99
+    latency under Poisson arrivals, and sequential single-system calls on the same requests."""
+    import numpy as np
+    import torch
+
+    from torchff_b200.serving import Server, SystemSpec, autotune_atoms_per_cell
+    from torchff_b200.system import FixedChargeSystem
+    from torchff_b200.water import serving_water_box
+
+    rng = np.random.default_rng(seed)
+    n_waters = np.exp(rng.uniform(math.log(64), math.log(4000), n_requests)).astype(int)
+    boxes = [serving_water_box(int(n), seed=seed * 100_003 + k) for k, n in enumerate(n_waters)]
+    specs = [SystemSpec.from_water_box(w) for w in boxes]
+    alpha, rc = boxes[0].alpha, 0.9
+    atoms = np.array([s.natoms for s in specs])
+    apc, tune_ms = autotune_atoms_per_cell(specs[:64], rc, alpha)
+    lanes, per_batch, budget = 3, 256, 6 << 30
+    srv = Server(rc, alpha, torch.float32, lanes=lanes, max_systems_per_batch=per_batch, hbm_budget_bytes=budget,
+                 atoms_per_cell=apc, device=device)
+
+    def run(rate):
+        """Submit every request (all at once for rate None, else Poisson arrivals); latencies."""
+        t0 = time.perf_counter()
+        arrivals = None if rate is None else np.cumsum(np.random.default_rng(seed + 7).exponential(1.0 / rate,
+                                                                                                n_requests))
+        s0 = srv.now()
+        reqs = []
+        for k, sp in enumerate(specs):
+            if arrivals is not None:
+                while time.perf_counter() - t0 < arrivals[k]:
+                    pass
+            reqs.append(srv.submit(sp))
+        srv.drain()
+        times = np.array([r.times() for r in reqs])
+        for r in reqs:
+            r.release()
+        lat = (times[:, 2] - times[:, 0]) * 1e3
+        span = times[:, 2].max() - s0
+        return reqs, {"systems_per_s": round(n_requests / span, 1), "p50_ms": round(float(np.median(lat)), 3),
+                      "p99_ms": round(float(np.percentile(lat, 99)), 3), "makespan_s": round(float(span), 4)}
+
+    run(None)  # warm-up: cuFFT plans for every grid size and batch count that shows up
+    b0 = srv.stats()["batches"]
+    reqs, sat = run(None)
+    st = srv.stats()
+    sat.update({"batches": st["batches"] - b0, "max_batch_systems": st["max_batch_systems"],
+                "max_lanes_in_flight": st["max_lanes_in_flight"]})
+    poisson = []
+    for frac in (0.25, 0.5, 0.8):
+        rate = frac * sat["systems_per_s"]
+        _, r = run(rate)
+        r["offered_rate_per_s"] = round(rate, 1)
+        poisson.append(r)
+    # accuracy of served results against FP64 single-system evaluations
+    errs = []
+    for k in range(0, n_requests, max(1, n_requests // 16)):
+        wb = boxes[k]
+        ref = FixedChargeSystem.from_water_box(wb, dtype=torch.float64, device=device).evaluate(
+            torch.tensor(wb.coords, dtype=torch.float64, device=device),
+            torch.tensor(wb.box, dtype=torch.float64, device=device))["forces"].cpu().numpy()
+        f = reqs[k].forces
+        errs.append(float(np.sqrt(np.mean((f - ref) ** 2)) / np.sqrt(np.mean(ref ** 2))))
+    stats = srv.stats()
+    srv.close()
+    # sequential single-system calls: prebuilt systems (evaluation only), and plain calls
+    # that set each system up per request (what a per-system API user does)
+    nseq = min(128, n_requests)
+    prebuilt = [FixedChargeSystem.from_water_box(boxes[k], dtype=torch.float32, device=device) for k in range(nseq)]
+    host = [(np.ascontiguousarray(boxes[k].coords), np.ascontiguousarray(boxes[k].box),
+             np.zeros_like(boxes[k].coords)) for k in range(nseq)]
+    for sy, (x, b, f) in zip(prebuilt, host):
+        sy.evaluate_host(x, b, f)
+    t0 = time.perf_counter()
+    for sy, (x, b, f) in zip(prebuilt, host):
+        sy.evaluate_host(x, b, f)
+    t_pre = (time.perf_counter() - t0) / nseq
+    del prebuilt
+    nplain = min(64, n_requests)
+    t0 = time.perf_counter()
+    for k in range(nseq, nseq + nplain):
+        wb = boxes[k % n_requests]
+        sy = FixedChargeSystem.from_water_box(wb, dtype=torch.float32, device=device)
+        sy.evaluate_host(np.ascontiguousarray(wb.coords), np.ascontiguousarray(wb.box), np.zeros_like(wb.coords))
+        del sy
+    t_plain = (time.perf_counter() - t0) / nplain
+    # the sequential samples hold the same size distribution; scale by mean atoms
+    return {
+        "workload": WORKLOAD_TEXT["serving"],
+        "requests": n_requests, "atoms_total": int(atoms.sum()), "atoms_mean": round(float(atoms.mean()), 1),
+        "server": {"lanes": lanes, "max_systems_per_batch": per_batch, "hbm_budget_bytes": budget,
+                   "lane_max_atoms": stats["lane_max_atoms"], "lane_device_bytes": stats["lane_device_bytes"],
+                   "atoms_per_cell": apc, "autotune_ms": {str(k): round(v, 3) for k, v in tune_ms.items()}},
+        "saturation": sat,
+        "poisson": poisson,
+        "sequential_prebuilt": {"us_per_system": round(t_pre * 1e6, 1), "systems_per_s": round(1.0 / t_pre, 1),
+                                "sample": f"first {nseq} requests, FixedChargeSystem.evaluate_host on systems "
+                                          "created beforehand (one CUDA-graph replay + copies per call)"},
+        "sequential_plain_calls": {"us_per_system": round(t_plain * 1e6, 1),
+                                   "systems_per_s": round(1.0 / t_plain, 1),
+                                   "sample": f"{nplain} requests, FixedChargeSystem created, evaluated "
+                                             "(evaluate_host) and freed per request"},
+        "speedup_vs_prebuilt": round(sat["systems_per_s"] * t_pre, 2),
+        "speedup_vs_plain_calls": round(sat["systems_per_s"] * t_plain, 2),
+        "accuracy": {"max_force_rms_rel_vs_fp64": float(f"{max(errs):.3g}"), "requests_checked": len(errs)},
+        "precision": "mixed",
+    }
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -198,6 +351,9 @@ def run_ours(args):
     import torchff_b200  # noqa: F401
     from torchff_b200.system import FixedChargeSystem, StageTimer
 
+    if args.workload == "serving":
+        run_serving_line(args, device, rank, world)
+        return
     dtype = torch.float32 if args.precision == "mixed" else torch.float64
     wb = water_box(args.workload, seed=rank)
     system = FixedChargeSystem.from_water_box(wb, dtype=dtype, device=device)
@@ -334,6 +490,10 @@ def run_ours(args):
             },
             "clocks": clk,
         }
+        if world == 1 and not args.no_fp64 and dtype == torch.float32:
+            result["fp64"] = time_graph_evals(wb, torch.float64, device, min(args.steps, 500), args.warmup)
+        if world == 1 and not args.no_serving:
+            result["serving"] = run_serving(device, args.serving_requests)
         if world == 1 and not args.no_cpu_baseline:
             if args.workload == "water100k":
                 result["cpu_baseline"] = {"value": None, "unit": "evals/s", "cores": 0, "kind": "port",
@@ -349,6 +509,41 @@ def run_ours(args):
         print(json.dumps(result), flush=True)
 
 
+def run_serving_line(args, device, rank, world):
+    """--workload serving: one server per rank on its own requests (no collective on the data
+    path); value = the ranks' saturation throughputs summed."""
+    import torch
+    import torch.distributed as dist
+
+    res = run_serving(device, args.serving_requests, seed=rank)
+    v = torch.tensor([res["saturation"]["systems_per_s"], res["saturation"]["p99_ms"]], dtype=torch.float64,
+                     device=device)
+    if world > 1:
+        tot = v.clone()
+        dist.all_reduce(tot[:1], op=dist.ReduceOp.SUM)
+        dist.all_reduce(tot[1:], op=dist.ReduceOp.MAX)
+        v = tot
+    if rank == 0:
+        bytes_in = res["atoms_mean"] * (3 * 8 + 3 * 8 + 2 * 8) + 72
+        line = {
+            "metric": "serving systems/s (continuous batching, saturation)",
+            "value": round(float(v[0]), 1), "unit": "systems/s", "n_gpus": world, "steps": args.serving_requests,
+            "warmup": args.serving_requests, "ms_per_step": round(1e3 / float(v[0]), 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded TIP3P boxes)",
+            "config": {"workload": f"serving: {WORKLOAD_TEXT['serving']}", "parallelism": f"server per rank x{world}",
+                       "l2": "inputs of a batch (tens of MB) exceed nothing; each request is new data"},
+            "e2e": {"value": round(float(v[0]), 1), "unit": "systems/s",
+                    "h2d_bytes_per_step": int(bytes_in), "d2h_bytes_per_step": int(res["atoms_mean"] * 24 + 8),
+                    "path": "tff_server_submit of host arrays -> batched evaluation -> host energy/forces"},
+            "p99_ms_max_over_ranks": round(float(v[1]), 3),
+            "serving": res,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 # ---------------------------------------------------------------------------------------
 # reference arm: the CPU restatement of the reference's pure-torch path
 # ---------------------------------------------------------------------------------------
@@ -362,7 +557,15 @@ def _ref_eval(task):
     workload, seed = task
     from oracle import oracle as O
 
-    wb = water_box(workload, seed)
+    if workload == "serving":
+        import numpy as np
+
+        from torchff_b200.water import serving_water_box
+
+        n = np.exp(np.random.default_rng(seed).uniform(math.log(64), math.log(4000))).astype(int)
+        wb = serving_water_box(int(n), seed=seed)
+    else:
+        wb = water_box(workload, seed)
     t0 = time.perf_counter()
     O.fixed_charge_energy(wb.coords, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
                           wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid, 138.935456)
@@ -391,11 +594,14 @@ def run_reference(args):
         per = pool.map(_ref_eval, [(args.workload, i) for i in range(n_eval)])
         wall = time.perf_counter() - t0
     value = n_eval / wall
+    serving = args.workload == "serving"
     line = {
         "impl": "reference",
-        "metric": METRIC if args.workload == "water3000" else f"{args.workload} PME energy+force evals/s",
+        "metric": (METRIC if args.workload == "water3000" else
+                   "serving systems/s (continuous batching, saturation)" if serving else
+                   f"{args.workload} PME energy+force evals/s"),
         "value": round(value, 4),
-        "unit": "evals/s",
+        "unit": "systems/s" if serving else "evals/s",
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
@@ -409,10 +615,12 @@ def run_reference(args):
                    "path": "numpy restatement of the reference pure-torch path (O(N^2) pair search, LJ type "
                            "tables, real-space Ewald with exclusion correction, PME), analytic forces",
                    "parallelism": f"{workers} host processes, one evaluation each at a time"},
-        "cpu_baseline": {"value": round(value, 4), "unit": "evals/s", "cores": workers, "kind": "port",
+        "cpu_baseline": {"value": round(value, 4), "unit": "systems/s" if serving else "evals/s", "cores": workers,
+                         "kind": "port",
                          "sample": f"{n_eval} full evaluations (of {args.steps} requested steps, bounded to ~90 s) "
                                    f"spread over {workers} single-thread processes"},
-        "e2e": {"value": round(value, 4), "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": round(value, 4), "unit": "systems/s" if serving else "evals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 

@@ -42,7 +42,8 @@ enum tff_status {
   TFF_ERR_CUDA = 2,        /* a CUDA runtime call failed */
   TFF_ERR_CUFFT = 3,       /* a cuFFT call failed */
   TFF_ERR_WORKSPACE = 4,   /* workspace too small */
-  TFF_ERR_CAPACITY = 5     /* a fixed-capacity list overflowed (see tff_system_status) */
+  TFF_ERR_CAPACITY = 5,    /* a fixed-capacity list overflowed (see tff_system_status) */
+  TFF_ERR_TIMEOUT = 6      /* a wait on the server ran out of time */
 };
 
 int tff_version(void);
@@ -244,6 +245,111 @@ int tff_system_eval_timed(tff_system sys, const void *coords, const void *box, d
                           void *forces, tff_timer timer, tff_stream_t stream);
 /* Number of kernels of this library one tff_system_eval launches (cuFFT's excluded). */
 int tff_system_kernel_launches(tff_system sys);
+
+/* ------------------------------------------------------------------------------
+ * Batches: many independent periodic systems per evaluation (serving)
+ *
+ * No reference counterpart: the reference evaluates one system per call (its torch-sim
+ * wrapper, examples/tip3p/md_torchsim.py:113-140, rejects n_systems != 1). A batch object
+ * owns device memory for up to max_systems systems holding max_atoms atoms and
+ * max_grid_points PME grid points (sum of K^3) in total; every stage of an evaluation is
+ * one launch over all systems (each with its own box, cell grid and PME grid K), and each
+ * system's result is the one a single-system evaluation of the same dtype gives (mixed
+ * precision: bit-identical whatever else is in the batch). Same physics as tff_system_*;
+ * cutoff, Ewald alpha and the Coulomb constant are shared by the batch.
+ * Per system: 1 <= natoms <= 16384, 6 <= K <= 128.
+ * --------------------------------------------------------------------------- */
+typedef struct tff_batch_s *tff_batch;
+
+typedef struct tff_batch_desc {
+  int dtype;
+  int max_systems;
+  int64_t max_atoms;
+  int64_t max_grid_points;
+  double cutoff;
+  double ewald_alpha;
+  double coul_constant;
+  int max_cluster_neighbors;  /* 0 = 512, enough for any accepted system */
+  double atoms_per_cell;      /* cell grid occupancy target, 0 = 8 */
+} tff_batch_desc;
+
+/* Device bytes a batch with this description allocates (for admission planning). */
+size_t tff_batch_device_bytes(const tff_batch_desc *desc);
+int tff_batch_create(const tff_batch_desc *desc, tff_batch *batch);
+int tff_batch_destroy(tff_batch batch);
+/* natoms[nsys], pme_grid[nsys]: HOST arrays. Device arrays, systems one after another in
+ * caller order: coords (sum natoms, 3), boxes (nsys, 3, 3), charges / sigma / epsilon
+ * (sum natoms), excl (sum natoms, 8) int32 excluded partners as atom indices within
+ * their own system, -1 padded; out: energies (nsys) float64, forces (sum natoms, 3) in the batch dtype.
+ * The host part (system table, FFT grouping) runs in the call; the call returns once the
+ * work is enqueued. One evaluation at a time per batch object and stream. */
+int tff_batch_eval(tff_batch batch, int nsys, const int64_t *natoms, const int *pme_grid, const void *coords,
+                   const void *boxes, const void *charges, const void *sigma, const void *epsilon,
+                   const int *excl, double *energies, void *forces, tff_stream_t stream);
+int tff_batch_status(tff_batch batch, tff_stream_t stream, int *status);
+int tff_batch_kernel_launches(tff_batch batch);
+
+/* ------------------------------------------------------------------------------
+ * Server: continuous batching of requests over tff_batch (no reference counterpart)
+ *
+ * A worker thread keeps `lanes` batches in flight, each on its own stream with its own
+ * device memory (hbm_budget_bytes split evenly; a lane's capacity in atoms and PME grid
+ * points is the largest that fits its share). Whenever a lane is free and requests are
+ * queued, it takes as many as fit (in submission order) and evaluates them as one batch,
+ * so requests arriving while other batches run start as soon as a lane frees up, and
+ * the lanes' batches overlap on the device. Inputs are copied at submission; energy and
+ * forces (float64) are written to the request's host buffers when it completes.
+ * --------------------------------------------------------------------------- */
+typedef struct tff_server_s *tff_server;
+
+typedef struct tff_server_desc {
+  int dtype;
+  int lanes;                    /* batches in flight, 1..16 */
+  int max_systems_per_batch;
+  size_t hbm_budget_bytes;      /* device memory of all lanes together */
+  double grid_points_per_atom;  /* lane PME grid capacity per atom of capacity (water at 0.1 nm: ~12) */
+  double cutoff;
+  double ewald_alpha;
+  double coul_constant;
+  double atoms_per_cell;        /* cell grid occupancy target, 0 = 8 */
+} tff_server_desc;
+
+typedef struct tff_request {
+  int64_t natoms;               /* 1..16384 */
+  int pme_grid;                 /* K, 6..128 */
+  const double *coords;         /* host (natoms, 3) */
+  const double *box;            /* host (3, 3), rows are box vectors */
+  const double *charges;        /* host (natoms) */
+  const double *sigma;          /* host (natoms) */
+  const double *epsilon;        /* host (natoms) */
+  int64_t nexcl;                /* excluded pairs (i, j), system-local indices */
+  const int64_t *excl_pairs;    /* host (nexcl, 2) */
+  double *energy;               /* host out, written on completion */
+  double *forces;               /* host out (natoms, 3), written on completion */
+} tff_request;
+
+typedef struct tff_server_stats {
+  int64_t submitted, systems_launched, systems_done, batches;
+  int64_t max_batch_systems, max_batch_atoms, max_lanes_in_flight;
+  int64_t lane_max_atoms, lane_max_grid_points, lane_device_bytes;
+  double now;                   /* seconds since the server was created (the request clock) */
+} tff_server_stats;
+
+int tff_server_create(const tff_server_desc *desc, tff_server *server);
+/* Finishes the queued requests, then stops the worker and frees everything. */
+int tff_server_destroy(tff_server server);
+int tff_server_submit(tff_server server, const tff_request *request, int64_t *ticket);
+/* Blocks until the request is done (timeout_s < 0: no limit); returns its status. */
+int tff_server_wait(tff_server server, int64_t ticket, double timeout_s);
+int tff_server_poll(tff_server server, int64_t ticket, int *done);
+/* Submission, batch start and completion times of a request on the server clock. */
+int tff_server_request_times(tff_server server, int64_t ticket, double *t_submit, double *t_start,
+                             double *t_done);
+/* Forgets a finished request. */
+int tff_server_release(tff_server server, int64_t ticket);
+/* Blocks until every submitted request is done. */
+int tff_server_drain(tff_server server, double timeout_s);
+int tff_server_get_stats(tff_server server, tff_server_stats *stats);
 
 #ifdef __cplusplus
 }

@@ -104,3 +104,32 @@ def test_ops_reject_cpu_tensors():
     x = torch.zeros(4, 3, dtype=torch.float64)
     with pytest.raises(Exception):
         torch.ops.torchff.build_neighbor_list_nsquared(x, None, 0.5, -1, None, None, False)
+
+
+def test_batch_exclusion_table_layout():
+    from torchff_b200.serving import exclusion_table
+
+    pairs = np.array([[0, 1], [0, 2], [1, 2], [2, 1], [3, 3], [5, 4]])
+    tab = exclusion_table(6, pairs)
+    expect = {0: [1, 2], 1: [0, 2], 2: [0, 1], 3: [], 4: [5], 5: [4]}
+    for a, partners in expect.items():
+        row = tab[a]
+        assert list(row[: len(partners)]) == partners and np.all(row[len(partners):] == -1)
+    with pytest.raises(ValueError):
+        exclusion_table(10, np.array([[0, k] for k in range(1, 10)]))
+
+
+def test_batch_and_server_argument_checks_need_no_gpu():
+    import ctypes as C
+
+    from torchff_b200 import _lib
+
+    d = _lib.BatchDesc(0, 64, 200_000, 2_000_000, 0.9, 2.92, 138.935456, 0, 0.0)
+    small = _lib.lib.tff_batch_device_bytes(C.byref(d))
+    d.max_atoms = 400_000
+    assert _lib.lib.tff_batch_device_bytes(C.byref(d)) > small > 0
+    h = C.c_void_p()
+    bad = _lib.ServerDesc(0, 0, 16, 1 << 30, 16.0, 0.9, 2.92, 138.935456, 0.0)  # lanes = 0
+    assert _lib.lib.tff_server_create(C.byref(bad), C.byref(h)) == 1
+    bad = _lib.BatchDesc(0, 64, 200_000, 2_000_000, 0.9, 2.92, 138.935456, 0, 100.0)  # atoms_per_cell
+    assert _lib.lib.tff_batch_create(C.byref(bad), C.byref(h)) == 1

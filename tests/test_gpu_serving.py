@@ -1,0 +1,134 @@
+"""Batched evaluation (tff_batch) and the continuous-batching server (tff_server).
+
+Each system of a batch must give the single-system result. The cluster lists and the
+fixed-point real-space sums are the same whatever else is in the batch; the reciprocal
+part differs only by the FP32 rounding of cuFFT, which runs the grids of equal size as one
+batched transform (a grid's rounding can depend on the batch count of its plan).
+Tolerances for "same system, other company": energy 1e-9 relative, forces 1e-6 of the
+largest force component.
+FP64 batches match the FP64 oracle to 1e-10 (energy) and 1e-8 (forces). The request sizes
+include boxes shorter than twice the cutoff (64 and 150 waters), evaluated with the
+minimum-image convention like the single-system path and the oracle.
+"""
+import numpy as np
+import pytest
+import torch
+
+from gpu_util import rel, rel_max, t
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RC = 0.9
+NS = [64, 150, 333, 900, 2500, 4000]
+
+
+def _boxes(ns, seed0=0):
+    from torchff_b200.serving import SystemSpec
+    from torchff_b200.water import serving_water_box
+
+    wbs = [serving_water_box(n, seed=seed0 + k) for k, n in enumerate(ns)]
+    return wbs, [SystemSpec.from_water_box(w) for w in wbs]
+
+
+def _single(wb, dtype):
+    from torchff_b200.system import FixedChargeSystem
+
+    s = FixedChargeSystem.from_water_box(wb, dtype=dtype)
+    return s.evaluate(t(wb.coords, dtype), t(wb.box, dtype))
+
+
+def _evaluator(dtype, wbs):
+    from torchff_b200.serving import BatchEvaluator
+
+    return BatchEvaluator(RC, wbs[0].alpha, dtype, max_systems=32, max_atoms=100_000, max_grid_points=2_000_000)
+
+
+@pytest.fixture(scope="module")
+def mixed_boxes():
+    return _boxes(NS)
+
+
+def test_batch_matches_single_system_mixed(mixed_boxes):
+    wbs, specs = mixed_boxes
+    ev = _evaluator(torch.float32, wbs)
+    e, f = ev.evaluate(specs)
+    torch.cuda.synchronize()
+    assert ev.status() == 0
+    for k, wb in enumerate(wbs):
+        ref = _single(wb, torch.float32)
+        assert rel(e[k].item(), ref["energy"].item()) < 1e-9, wb.n_waters
+        assert rel_max(f[k], ref["forces"]) < 1e-6, wb.n_waters
+
+
+def test_batch_fp64_matches_oracle():
+    wbs, specs = _boxes([64, 150, 333], seed0=10)
+    ev = _evaluator(torch.float64, wbs)
+    e, f = ev.evaluate(specs)
+    torch.cuda.synchronize()
+    for k, wb in enumerate(wbs):
+        ref = O.fixed_charge_energy(wb.coords, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
+                                    wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
+                                    138.935456)
+        assert rel(e[k].item(), ref["total"]) < 1e-10, wb.n_waters
+        assert rel_max(f[k], -ref["grad_coords"]) < 1e-8, wb.n_waters
+
+
+def test_result_alone_equals_result_in_a_mix(mixed_boxes):
+    wbs, specs = mixed_boxes
+    ev = _evaluator(torch.float32, wbs)
+    target = specs[3]
+    e1, f1 = ev.evaluate([target])
+    e1, f1 = e1.clone(), f1[0].clone()
+    # a mix with the same K twice more (a batched FFT group of 3) and other sizes around it
+    others, _ = _boxes([900, 900, 64, 4000, 150], seed0=50)
+    from torchff_b200.serving import SystemSpec
+
+    mix = [SystemSpec.from_water_box(w) for w in others[:2]] + [target] + [SystemSpec.from_water_box(w) for w in others[2:]]
+    assert all(s.pme_grid == target.pme_grid for s in mix[:3])
+    e2, f2 = ev.evaluate(mix)
+    torch.cuda.synchronize()
+    assert rel(e2[2].item(), e1.item()) < 1e-9
+    assert rel_max(f2[2], f1) < 1e-6
+
+
+def test_server_results_match_batch_and_timestamps():
+    from torchff_b200.serving import Server
+
+    rng = np.random.default_rng(5)
+    ns = np.exp(rng.uniform(np.log(64), np.log(2000), 40)).astype(int)
+    wbs, specs = _boxes(ns, seed0=100)
+    srv = Server(RC, wbs[0].alpha, torch.float32, lanes=2, max_systems_per_batch=16, hbm_budget_bytes=2 << 30)
+    reqs = [srv.submit(s) for s in specs]
+    srv.drain(timeout=120)
+    st = srv.stats()
+    assert st["systems_done"] == len(specs) and st["batches"] >= 3 and st["max_batch_systems"] <= 16
+    ev = _evaluator(torch.float32, wbs)
+    for k in range(0, len(specs), 7):
+        e, f = ev.evaluate([specs[k]])
+        torch.cuda.synchronize()
+        en, fn = reqs[k].wait()
+        assert rel(en, e.item()) < 1e-9
+        assert rel_max(fn, f[0]) < 1e-6
+    for r in reqs:
+        a, b, c = r.times()
+        assert a <= b <= c
+        r.release()
+    srv.close()
+
+
+def test_server_request_alone_equals_request_in_a_mix(mixed_boxes):
+    from torchff_b200.serving import Server
+
+    wbs, specs = mixed_boxes
+    srv = Server(RC, wbs[0].alpha, torch.float32, lanes=3, max_systems_per_batch=8, hbm_budget_bytes=2 << 30)
+    alone = srv.submit(specs[4])
+    ea, fa = alone.wait(timeout=60)
+    fa = fa.copy()
+    others, ospecs = _boxes([120, 700, 2000, 64, 3000, 400, 1000, 250], seed0=200)
+    reqs = [srv.submit(s) for s in ospecs[:4]] + [srv.submit(specs[4])] + [srv.submit(s) for s in ospecs[4:]]
+    eb, fb = reqs[4].wait(timeout=60)
+    srv.drain(timeout=60)
+    assert rel(eb, ea) < 1e-9
+    assert rel_max(fb, fa) < 1e-6
+    srv.close()

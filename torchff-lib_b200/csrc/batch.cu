@@ -1,0 +1,521 @@
+// Batched evaluation of many independent periodic systems (the serving path): every stage
+// is one launch over all systems of the batch.
+//
+//   main stream : batch_sort (one block per system: its own box facts and Hilbert cell
+//                 grid) -> cluster bounds -> cluster neighbours -> sorted parameters ->
+//                 tile kernel -> [join] -> finalize (forces, one energy per system)
+//   PME stream  : spread (blockIdx.y = system) -> [fixed point -> FP32] -> R2C FFT per
+//                 group of equal K -> convolution -> C2R FFT per group -> gather
+//
+// Systems are laid out one after another in every array; the cluster lists never leave a
+// system, and every per-system reduction runs over a block count that depends on that
+// system alone, so a system's result does not depend on what else is in the batch. The
+// PME grids are ordered by K so that each group of equal K is one batched cuFFT call (the
+// group is split into power-of-two counts, whose plans are cached).
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <tuple>
+#include <utility>
+#include <vector>
+
+#include "tile.cuh"
+
+namespace tff {
+namespace {
+
+constexpr int kBatchMaxK = 128;
+
+// Grid distances inside the batch: every real grid starts on a 256-byte boundary and every
+// complex grid on a 256-byte (FP32) boundary, as cuFFT wants aligned transform inputs.
+inline int64_t real_dist(int K) { return ((int64_t)K * K * K + 63) / 64 * 64; }
+inline int64_t cplx_dist(int K) { return ((int64_t)K * K * (K / 2 + 1) + 31) / 32 * 32; }
+
+// Offset of grid K's moduli (xmod (K), ymod (K), zmod (K/2+1)) in the moduli table.
+inline int moduli_offset(int K) {
+  int off = 0;
+  for (int k = 6; k < K; ++k) off += 2 * k + k / 2 + 1;
+  return off;
+}
+
+struct BatchLayout {
+  int64_t atoms, systems, clusters, supers, grid;
+  int cap;
+  size_t sys, status, boxinfo, cl_sys, sup_sys, sidx, inv, pos, frac, bc, bh, sbc, sbh, nbr, ncount, itemoff, items;
+  size_t lj, exslot, acc, e_tile;
+  size_t fix, real, cplx, partials, tickets, e_pme, pme_grad, pme_phi, moduli;
+  size_t bytes;
+};
+
+inline BatchLayout batch_layout(int dtype, int64_t max_atoms, int64_t max_systems, int64_t max_grid, int cap) {
+  BatchLayout L{};
+  L.atoms = max_atoms;
+  L.systems = max_systems;
+  L.clusters = max_atoms / kWarp + max_systems;
+  L.supers = L.clusters / kSuper + max_systems;
+  L.grid = max_grid;
+  L.cap = cap;
+  const size_t ts = dtype == TFF_F64 ? 8 : 4;
+  const int64_t slots = L.clusters * kWarp;
+  Carver c(nullptr);
+  auto take = [&](size_t bytes) {
+    c.take<char>(bytes);
+    return c.off - bytes;
+  };
+  L.sys = take(max_systems * sizeof(BatchSys));
+  L.status = take(64 * sizeof(unsigned));
+  L.boxinfo = take(max_systems * kInfoStride * sizeof(double));
+  L.cl_sys = take(L.clusters * sizeof(int));
+  L.sup_sys = take(L.supers * sizeof(int));
+  L.sidx = take(slots * sizeof(int));
+  L.inv = take(max_atoms * sizeof(int));
+  L.pos = take(slots * 4 * ts);
+  L.frac = take(slots * 4 * ts);
+  L.bc = take(L.clusters * 4 * ts);
+  L.bh = take(L.clusters * 4 * ts);
+  L.sbc = take(L.supers * 4 * ts);
+  L.sbh = take(L.supers * 4 * ts);
+  L.nbr = take((size_t)L.clusters * cap * sizeof(int));
+  L.ncount = take(L.clusters * sizeof(int));
+  L.itemoff = take((L.clusters + 1) * sizeof(int));
+  L.items = take((size_t)L.clusters * ((cap + kItemTiles - 1) / kItemTiles) * sizeof(int));
+  L.lj = take(slots * 2 * ts);
+  L.exslot = take(slots * kMaxExcl * sizeof(int));
+  L.acc = take(slots * 4 * 8);  // gx (3 per slot) + gq, fixed point or double
+  L.e_tile = take(2 * max_systems * 8);
+  const int64_t grid_cap = max_grid + 64 * max_systems;  // padding of real_dist / cplx_dist
+  L.fix = take(grid_cap * 8);
+  L.real = take(dtype == TFF_F64 ? 0 : grid_cap * ts);
+  L.cplx = take(grid_cap * 2 * ts);  // K*K*(K/2+1) <= K^3 complex points per system
+  L.partials = take((size_t)max_systems * kBatchPmeMaxBlocks * sizeof(double));
+  L.tickets = take(2 * max_systems * sizeof(unsigned));
+  L.e_pme = take(2 * max_systems * sizeof(double));
+  L.pme_grad = take(3 * max_atoms * ts);
+  L.pme_phi = take(max_atoms * ts);
+  L.moduli = take((size_t)moduli_offset(kBatchMaxK + 1) * ts);
+  L.bytes = c.bytes();
+  return L;
+}
+
+struct FftGroup {
+  int K;
+  int64_t grid_off, cplx_off;
+  int count;
+};
+
+// Batched cuFFT plans of the process, shared by every batch object: (device, dtype, K,
+// count) -> (R2C, C2R, work bytes). Plans run without their own work area; each batch
+// object passes its own, so batches on different streams can use one plan concurrently.
+struct PlanEntry {
+  cufftHandle r2c, c2r;
+  size_t work;
+};
+std::mutex g_plan_mu;
+std::map<std::tuple<int, int, int, int>, PlanEntry> g_plans;
+
+int shared_plans(int dtype, int K, int count, PlanEntry &out) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, dtype, K, count);
+  std::lock_guard<std::mutex> g(g_plan_mu);
+  auto it = g_plans.find(key);
+  if (it != g_plans.end()) {
+    out = it->second;
+    return TFF_OK;
+  }
+  const bool f64 = dtype == TFF_F64;
+  int n[3] = {K, K, K}, cn[3] = {K, K, K / 2 + 1};
+  const int rd = (int)real_dist(K), cd = (int)cplx_dist(K);
+  cufftHandle h[2] = {0, 0};
+  size_t work[2] = {0, 0};
+  for (int d = 0; d < 2; ++d) {
+    cufftResult r = cufftCreate(&h[d]);
+    if (r == CUFFT_SUCCESS) r = cufftSetAutoAllocation(h[d], 0);
+    if (r == CUFFT_SUCCESS) {
+      if (d == 0)
+        r = cufftMakePlanMany(h[d], 3, n, n, 1, rd, cn, 1, cd, f64 ? CUFFT_D2Z : CUFFT_R2C, count, &work[d]);
+      else
+        r = cufftMakePlanMany(h[d], 3, n, cn, 1, cd, n, 1, rd, f64 ? CUFFT_Z2D : CUFFT_C2R, count, &work[d]);
+    }
+    if (r != CUFFT_SUCCESS) {
+      for (int e = 0; e <= d; ++e)
+        if (h[e]) cufftDestroy(h[e]);
+      return pme_cufft_fail(r, "batched plan");
+    }
+  }
+  out = PlanEntry{h[0], h[1], std::max(work[0], work[1])};
+  g_plans[key] = out;
+  return TFF_OK;
+}
+
+}  // namespace
+}  // namespace tff
+
+using namespace tff;
+
+struct tff_batch_s {
+  tff_batch_desc desc;
+  BatchLayout L;
+  char *ws = nullptr;
+  BatchSys *table = nullptr;       // pinned host copy of the system table
+  cudaEvent_t table_ev = nullptr;  // the table upload of the previous evaluation
+  cudaStream_t pme_stream = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  void *fft_work = nullptr;        // this batch's cuFFT work area
+  size_t fft_work_bytes = 0;
+  std::vector<BatchSys> host_sys;
+  std::vector<FftGroup> groups;
+  int device = 0;
+};
+
+namespace tff {
+namespace {
+
+void free_batch(tff_batch b) {
+  if (!b) return;
+  if (b->fft_work) cudaFree(b->fft_work);
+  if (b->ws) cudaFree(b->ws);
+  if (b->table) cudaFreeHost(b->table);
+  if (b->table_ev) cudaEventDestroy(b->table_ev);
+  if (b->pme_stream) cudaStreamDestroy(b->pme_stream);
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+  if (b->join_ev) cudaEventDestroy(b->join_ev);
+  delete b;
+}
+
+// Plans for `count` contiguous K^3 grids (created on first use, process-wide) with this
+// batch's work area grown to fit; growing waits for the batch's own streams.
+int get_plans(tff_batch b, int K, int count, cufftHandle &r2c, cufftHandle &c2r) {
+  PlanEntry p;
+  int st = shared_plans(b->desc.dtype, K, count, p);
+  if (st != TFF_OK) return st;
+  const size_t need = std::max<size_t>(256, p.work);
+  if (need > b->fft_work_bytes) {
+    TFF_CUDA(cudaStreamSynchronize(b->pme_stream));
+    if (b->fft_work) TFF_CUDA(cudaFree(b->fft_work));
+    b->fft_work = nullptr;
+    b->fft_work_bytes = 0;
+    TFF_CUDA(cudaMalloc(&b->fft_work, need));
+    b->fft_work_bytes = need;
+  }
+  r2c = p.r2c;
+  c2r = p.c2r;
+  return TFF_OK;
+}
+
+// One FFT direction over every group; a group of count c runs as the binary digits of c.
+template <class T>
+int run_ffts(tff_batch b, bool forward, T *real, typename CplxOf<T>::type *cplx, cudaStream_t s) {
+  for (const FftGroup &g : b->groups) {
+    int64_t goff = g.grid_off, coff = g.cplx_off;
+    const int64_t rstep = real_dist(g.K), cstep = cplx_dist(g.K);
+    for (int bit = 30; bit >= 0; --bit) {
+      const int cnt = 1 << bit;
+      if (!(g.count & cnt)) continue;
+      cufftHandle r2c, c2r;
+      int st = get_plans(b, g.K, cnt, r2c, c2r);
+      if (st != TFF_OK) return st;
+      cufftHandle h = forward ? r2c : c2r;
+      // stream, work area and launch of a shared plan in one critical section
+      std::lock_guard<std::mutex> guard(g_plan_mu);
+      cufftResult r = cufftSetStream(h, s);
+      if (r == CUFFT_SUCCESS) r = cufftSetWorkArea(h, b->fft_work);
+      if (r != CUFFT_SUCCESS) return pme_cufft_fail(r, "cufftSetStream/WorkArea");
+      if (sizeof(T) == 4) {
+        r = forward ? cufftExecR2C(h, reinterpret_cast<cufftReal *>(real + goff), reinterpret_cast<cufftComplex *>(cplx + coff))
+                    : cufftExecC2R(h, reinterpret_cast<cufftComplex *>(cplx + coff), reinterpret_cast<cufftReal *>(real + goff));
+      } else {
+        r = forward ? cufftExecD2Z(h, reinterpret_cast<cufftDoubleReal *>(real + goff),
+                                   reinterpret_cast<cufftDoubleComplex *>(cplx + coff))
+                    : cufftExecZ2D(h, reinterpret_cast<cufftDoubleComplex *>(cplx + coff),
+                                   reinterpret_cast<cufftDoubleReal *>(real + goff));
+      }
+      if (r != CUFFT_SUCCESS) return pme_cufft_fail(r, forward ? "batched forward FFT" : "batched inverse FFT");
+      goff += cnt * rstep;
+      coff += cnt * cstep;
+    }
+  }
+  return TFF_OK;
+}
+
+template <class T>
+int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme_grid, const T *x, const T *boxes,
+                    const T *q, const T *sigma, const T *eps, const int *excl, double *energies, T *forces,
+                    cudaStream_t s) {
+  using S = typename Acc<T>::S;
+  const BatchLayout &L = b->L;
+  // --- host: system table, grid order, FFT groups
+  auto &hs = b->host_sys;
+  hs.assign(nsys, BatchSys{});
+  int64_t ao = 0, co = 0, so = 0, go = 0, xo = 0, max_pb = 1;
+  for (int i = 0; i < nsys; ++i) {
+    const int64_t n = natoms[i];
+    const int K = pme_grid[i];
+    TFF_ARG(n >= 1 && n <= kBatchMaxAtoms, "system %d: natoms %lld outside [1, %d]", i, (long long)n, kBatchMaxAtoms);
+    TFF_ARG(K >= 6 && K <= kBatchMaxK, "system %d: PME grid %d outside [6, %d]", i, K, kBatchMaxK);
+    BatchSys &y = hs[i];
+    y.atom_off = ao;
+    y.natoms = n;
+    y.ncl = (n + kWarp - 1) / kWarp;
+    y.cl_off = co;
+    y.nsup = (y.ncl + kSuper - 1) / kSuper;
+    y.sup_off = so;
+    cell_grid(n, b->desc.atoms_per_cell, y.nc, y.bits);
+    TFF_ARG((1 << (3 * y.bits)) <= kBatchMaxKeys, "system %d: cell grid too fine", i);
+    y.K = K;
+    y.mod_off = moduli_offset(K);
+    const int64_t ncplx = (int64_t)K * K * (K / 2 + 1);
+    y.pme_blocks = (int)std::min<int64_t>(kBatchPmeMaxBlocks, std::max<int64_t>(1, (std::max(n * kLanesPerAtom, ncplx) + kPmeBlock - 1) / kPmeBlock));
+    max_pb = std::max<int64_t>(max_pb, y.pme_blocks);
+    ao += n;
+    co += y.ncl;
+    so += y.nsup;
+  }
+  TFF_ARG(ao <= L.atoms, "batch holds %lld atoms; capacity %lld", (long long)ao, (long long)L.atoms);
+  std::vector<int> order(nsys);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return hs[a].K < hs[c].K; });
+  b->groups.clear();
+  for (int i : order) {
+    BatchSys &y = hs[i];
+    y.grid_off = go;
+    y.cplx_off = xo;
+    if (b->groups.empty() || b->groups.back().K != y.K) b->groups.push_back(FftGroup{y.K, go, xo, 0});
+    b->groups.back().count++;
+    go += real_dist(y.K);
+    xo += cplx_dist(y.K);
+  }
+  TFF_ARG(go <= L.grid + 64 * L.systems, "batch holds %lld PME grid points; capacity %lld", (long long)go,
+          (long long)L.grid);
+  const int64_t ncl = co, nsup = so, npad = co * kWarp, total_atoms = ao, total_grid = go;
+
+  // --- device pointers
+  char *w = b->ws;
+  ClusterData<T> cd{};
+  using V = typename V4<T>::type;
+  cd.status = reinterpret_cast<unsigned *>(w + L.status);
+  cd.sidx = reinterpret_cast<int *>(w + L.sidx);
+  cd.inv = reinterpret_cast<int *>(w + L.inv);
+  cd.nbr = reinterpret_cast<int *>(w + L.nbr);
+  cd.ncount = reinterpret_cast<int *>(w + L.ncount);
+  cd.itemoff = reinterpret_cast<int *>(w + L.itemoff);
+  cd.items = reinterpret_cast<int *>(w + L.items);
+  cd.pos = reinterpret_cast<V *>(w + L.pos);
+  cd.frac = reinterpret_cast<V *>(w + L.frac);
+  cd.bc = reinterpret_cast<V *>(w + L.bc);
+  cd.bh = reinterpret_cast<V *>(w + L.bh);
+  cd.sbc = reinterpret_cast<V *>(w + L.sbc);
+  cd.sbh = reinterpret_cast<V *>(w + L.sbh);
+  cd.boxinfo = reinterpret_cast<double *>(w + L.boxinfo);
+  cd.cap = L.cap;
+  cd.natoms = total_atoms;
+  cd.nclusters = ncl;
+  cd.npad = npad;
+  cd.nsuper = nsup;
+  cd.sys = reinterpret_cast<const BatchSys *>(w + L.sys);
+  cd.cl_sys = reinterpret_cast<int *>(w + L.cl_sys);
+  cd.sup_sys = reinterpret_cast<int *>(w + L.sup_sys);
+
+  // --- upload the table (the pinned buffer is reused once the previous upload is done)
+  TFF_CUDA(cudaEventSynchronize(b->table_ev));
+  std::copy(hs.begin(), hs.end(), b->table);
+  TFF_CUDA(cudaMemcpyAsync(w + L.sys, b->table, nsys * sizeof(BatchSys), cudaMemcpyHostToDevice, s));
+  TFF_CUDA(cudaEventRecord(b->table_ev, s));
+  TFF_CUDA(cudaMemsetAsync(w + L.status, 0, 64 * sizeof(unsigned), s));
+  TFF_CUDA(cudaMemsetAsync(w + L.e_tile, 0, 2 * nsys * 8, s));
+  TFF_CUDA(cudaMemsetAsync(w + L.acc, 0, npad * 4 * 8, s));
+  const int sms = sm_count();
+
+  // --- PME on the side stream
+  TFF_CUDA(cudaEventRecord(b->fork_ev, s));
+  cudaStream_t ps = b->pme_stream;
+  TFF_CUDA(cudaStreamWaitEvent(ps, b->fork_ev, 0));
+  TFF_CUDA(cudaMemsetAsync(w + L.fix, 0, total_grid * 8, ps));
+  TFF_CUDA(cudaMemsetAsync(w + L.tickets, 0, 2 * nsys * sizeof(unsigned), ps));
+  const BatchSys *dsys = cd.sys;
+  double *partials = reinterpret_cast<double *>(w + L.partials);
+  unsigned *tickets = reinterpret_cast<unsigned *>(w + L.tickets);
+  double *e_pme = reinterpret_cast<double *>(w + L.e_pme);
+  S *fix = reinterpret_cast<S *>(w + L.fix);
+  T *pme_grad = reinterpret_cast<T *>(w + L.pme_grad);
+  T *pme_phi = reinterpret_cast<T *>(w + L.pme_phi);
+  const dim3 pgrid((unsigned)max_pb, (unsigned)nsys);
+  batch_spread_kernel<T><<<pgrid, kPmeBlock, 0, ps>>>(dsys, x, q, boxes, fix);
+  TFF_LAUNCHED();
+  T *real;
+  if (sizeof(T) == 4) {
+    real = reinterpret_cast<T *>(w + L.real);
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((total_grid + 255) / 256, sms * 8));
+    pme_fix_to_real_kernel<<<nb, 256, 0, ps>>>(reinterpret_cast<unsigned long long *>(fix),
+                                               reinterpret_cast<float *>(real), total_grid);
+    TFF_LAUNCHED();
+  } else {
+    real = reinterpret_cast<T *>(fix);
+  }
+  auto *cplx = reinterpret_cast<typename CplxOf<T>::type *>(w + L.cplx);
+  int st = run_ffts<T>(b, true, real, cplx, ps);
+  if (st != TFF_OK) return st;
+  batch_convolve_kernel<T><<<pgrid, kPmeBlock, 0, ps>>>(dsys, cplx, boxes, b->desc.ewald_alpha,
+                                                        reinterpret_cast<const T *>(w + L.moduli), partials, tickets,
+                                                        e_pme);
+  TFF_LAUNCHED();
+  if ((st = run_ffts<T>(b, false, real, cplx, ps)) != TFF_OK) return st;
+  batch_gather_kernel<T><<<pgrid, kPmeBlock, 0, ps>>>(dsys, x, q, boxes, real, b->desc.ewald_alpha, pme_phi, pme_grad,
+                                                      partials, tickets, e_pme);
+  TFF_LAUNCHED();
+  TFF_CUDA(cudaEventRecord(b->join_ev, ps));
+
+  // --- real space on the caller stream
+  batch_sort_kernel<T><<<(int)std::min<int64_t>(nsys, 2 * sms), kBatchSortThreads, kBatchSortSmem, s>>>(x, q, boxes,
+                                                                                                     nsys, cd);
+  TFF_LAUNCHED();
+  cluster_bounds_kernel<T><<<(int)std::max<int64_t>(1, std::min<int64_t>(nsup, 2 * sms)), kWarp * kSuper, 0, s>>>(cd);
+  TFF_LAUNCHED();
+  const int nb_cl = (int)std::max<int64_t>(1, std::min<int64_t>((ncl + 3) / 4, sms * 16));
+  cluster_neighbors_kernel<T><<<nb_cl, 128, 0, s>>>(cd, b->desc.cutoff, 0);
+  TFF_LAUNCHED();
+  auto *lj = reinterpret_cast<typename V2<T>::type *>(w + L.lj);
+  int *exslot = reinterpret_cast<int *>(w + L.exslot);
+  {
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((npad + 255) / 256, sms * 8));
+    sorted_params_kernel<T><<<nb, 256, 0, s>>>(cd, sigma, eps, excl, lj, exslot);
+    TFF_LAUNCHED();
+  }
+  S *gx = reinterpret_cast<S *>(w + L.acc);
+  S *gq = gx + 3 * npad;
+  S *e_tile = reinterpret_cast<S *>(w + L.e_tile);
+  {
+    TileArgs<T> A;
+    A.cl = cd;
+    A.lj = lj;
+    A.exslot = exslot;
+    A.gx = gx;
+    A.gq = gq;
+    A.rc = b->desc.cutoff;
+    A.alpha = b->desc.ewald_alpha;
+    A.kc = b->desc.coul_constant;
+    A.energies = e_tile;
+    const int64_t max_items = ncl * ((L.cap + kItemTiles - 1) / kItemTiles);
+    constexpr int NW = TileCfg<T>::NW;
+    const int nbt = (int)std::max<int64_t>(1, std::min<int64_t>((max_items + NW - 1) / NW, (int64_t)sms * 48 / NW));
+    tile_kernel<T><<<nbt, NW * kWarp, 0, s>>>(A);
+    TFF_LAUNCHED();
+  }
+  TFF_CUDA(cudaStreamWaitEvent(s, b->join_ev, 0));
+  const int nbf = (int)std::max<int64_t>(1, std::min<int64_t>((total_atoms + 255) / 256, sms * 8));
+  finalize_kernel<T><<<nbf, 256, 0, s>>>(cd, gx, gq, pme_grad, pme_phi, forces, (double *)nullptr, (T *)nullptr,
+                                         e_tile, e_pme, b->desc.coul_constant, energies, (double *)nullptr, nsys);
+  TFF_LAUNCHED();
+  return TFF_OK;
+}
+
+template <class T>
+int set_sort_smem() {
+  TFF_CUDA(cudaFuncSetAttribute(batch_sort_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kBatchSortSmem));
+  return TFF_OK;
+}
+
+}  // namespace
+}  // namespace tff
+
+extern "C" {
+
+size_t tff_batch_device_bytes(const tff_batch_desc *desc) {
+  if (!desc) return 0;
+  const int cap = desc->max_cluster_neighbors > 0 ? desc->max_cluster_neighbors : kBatchMaxAtoms / kWarp;
+  return batch_layout(desc->dtype, desc->max_atoms, desc->max_systems, desc->max_grid_points, cap).bytes;
+}
+
+int tff_batch_create(const tff_batch_desc *desc, tff_batch *out) {
+  TFF_ARG(desc != nullptr && out != nullptr, "desc/out is NULL");
+  TFF_ARG(desc->dtype == TFF_F32 || desc->dtype == TFF_F64, "dtype must be TFF_F32 or TFF_F64");
+  TFF_ARG(desc->max_systems >= 1 && desc->max_systems <= 65535, "max_systems must be in [1, 65535]");
+  TFF_ARG(desc->max_atoms >= 1 && desc->max_atoms < ((int64_t)1 << 30), "max_atoms out of range");
+  TFF_ARG(desc->max_grid_points >= 216, "max_grid_points must be at least 6^3");
+  TFF_ARG(desc->cutoff > 0.0 && desc->ewald_alpha > 0.0, "cutoff and ewald_alpha must be positive");
+  TFF_ARG(desc->atoms_per_cell == 0.0 || (desc->atoms_per_cell >= 2.0 && desc->atoms_per_cell <= 64.0),
+          "atoms_per_cell must be 0 (default 8) or in [2, 64]");
+  auto *b = new tff_batch_s();
+  b->desc = *desc;
+  if (b->desc.atoms_per_cell == 0.0) b->desc.atoms_per_cell = 8.0;
+  // a system has at most kBatchMaxAtoms / 32 clusters, so the default cap cannot overflow
+  const int cap = desc->max_cluster_neighbors > 0 ? desc->max_cluster_neighbors : kBatchMaxAtoms / kWarp;
+  b->L = batch_layout(desc->dtype, desc->max_atoms, desc->max_systems, desc->max_grid_points, cap);
+  cudaGetDevice(&b->device);
+  cudaError_t e = cudaMalloc(&b->ws, b->L.bytes);
+  if (e == cudaSuccess) e = cudaMemset(b->ws, 0, b->L.bytes);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&b->table, desc->max_systems * sizeof(BatchSys));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->table_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->pme_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) {
+    // B-spline moduli of every grid size the batch accepts
+    std::vector<double> mod;
+    for (int K = 6; K <= kBatchMaxK; ++K) {
+      auto mx = host_moduli(K, K), mz = host_moduli(K, K / 2 + 1);
+      mod.insert(mod.end(), mx.begin(), mx.end());
+      mod.insert(mod.end(), mx.begin(), mx.end());
+      mod.insert(mod.end(), mz.begin(), mz.end());
+    }
+    if (desc->dtype == TFF_F64) {
+      e = cudaMemcpy(b->ws + b->L.moduli, mod.data(), mod.size() * 8, cudaMemcpyHostToDevice);
+    } else {
+      std::vector<float> mf(mod.begin(), mod.end());
+      e = cudaMemcpy(b->ws + b->L.moduli, mf.data(), mf.size() * 4, cudaMemcpyHostToDevice);
+    }
+  }
+  if (e != cudaSuccess) {
+    free_batch(b);
+    return cuda_fail(e, "batch set-up", __FILE__, __LINE__);
+  }
+  const int st = desc->dtype == TFF_F64 ? set_sort_smem<double>() : set_sort_smem<float>();
+  if (st != TFF_OK) {
+    free_batch(b);
+    return st;
+  }
+  *out = b;
+  return TFF_OK;
+}
+
+int tff_batch_destroy(tff_batch b) {
+  free_batch(b);
+  return TFF_OK;
+}
+
+int tff_batch_eval(tff_batch b, int nsys, const int64_t *natoms, const int *pme_grid, const void *coords,
+                   const void *boxes, const void *charges, const void *sigma, const void *epsilon, const int *excl,
+                   double *energies, void *forces, tff_stream_t stream) {
+  TFF_ARG(b != nullptr, "batch is NULL");
+  TFF_ARG(nsys >= 1 && nsys <= b->desc.max_systems, "nsys %d outside [1, %d]", nsys, b->desc.max_systems);
+  TFF_ARG(natoms && pme_grid && coords && boxes && charges && sigma && epsilon && excl && energies && forces,
+          "NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (b->desc.dtype == TFF_F32)
+    return batch_eval_impl<float>(b, nsys, natoms, pme_grid, (const float *)coords, (const float *)boxes,
+                                  (const float *)charges, (const float *)sigma, (const float *)epsilon, excl, energies,
+                                  (float *)forces, s);
+  return batch_eval_impl<double>(b, nsys, natoms, pme_grid, (const double *)coords, (const double *)boxes,
+                                 (const double *)charges, (const double *)sigma, (const double *)epsilon, excl,
+                                 energies, (double *)forces, s);
+}
+
+int tff_batch_status(tff_batch b, tff_stream_t stream, int *status) {
+  TFF_ARG(b != nullptr && status != nullptr, "batch/status is NULL");
+  unsigned v = 0;
+  TFF_CUDA(cudaMemcpyAsync(&v, b->ws + b->L.status, sizeof(unsigned), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  TFF_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  *status = (int)v;
+  return TFF_OK;
+}
+
+int tff_batch_kernel_launches(tff_batch b) {
+  if (!b) return 0;
+  // sort, bounds, neighbours, params, tile, finalize; spread, [to_real], convolve, gather
+  return 6 + (b->desc.dtype == TFF_F32 ? 4 : 3);
+}
+
+}  // extern "C"

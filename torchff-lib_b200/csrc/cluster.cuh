@@ -45,19 +45,26 @@ struct ClusterLayout {
   size_t zero_off, zero_bytes, bytes;
 };
 
+// Cell grid side (cells per box vector) and Hilbert bits for `natoms` atoms at about
+// `atoms_per_cell` atoms per cell. 8 is the default: runs of 32 atoms along the curve then
+// form the most compact clusters (fewest cluster pairs within the cutoff) among 2..32
+// atoms per cell on water boxes. From 16 cells per side up, the side is rounded to a power
+// of two: on a grid that only partly fills its 2^b key space the curve leaves and
+// re-enters the grid, and a 32-atom run across such a jump is not compact (small boxes
+// bound the damage).
+inline void cell_grid(int64_t natoms, double atoms_per_cell, int &nc, int &bits) {
+  const double g = cbrt((double)natoms / atoms_per_cell);
+  nc = g >= 16.0 ? (1 << (int)lround(log2(g))) : (int)floor(g);
+  nc = std::max(1, std::min(nc, 128));
+  bits = 0;
+  while ((1 << bits) < nc) ++bits;
+}
+
 inline ClusterLayout cluster_layout(int dtype, int64_t natoms, int cap) {
   ClusterLayout L;
   L.natoms = natoms;
-  // ~8 atoms per cell: runs of 32 atoms along the curve form the most compact clusters
-  // (fewest cluster pairs within the cutoff) among 2..32 atoms per cell on water boxes.
-  // From 16 cells per side up, the side is rounded to a power of two: on a grid that only
-  // partly fills its 2^b key space the curve leaves and re-enters the grid, and a 32-atom
-  // run across such a jump is not compact (small boxes bound the damage).
-  const double g = cbrt((double)natoms / 8.0);
-  int nc = g >= 16.0 ? (1 << (int)lround(log2(g))) : (int)floor(g);
-  nc = std::max(1, std::min(nc, 128));
-  int bits = 0;
-  while ((1 << bits) < nc) ++bits;
+  int nc, bits;
+  cell_grid(natoms, 8.0, nc, bits);
   L.nc = nc;
   L.bits = bits;
   L.nkeys = (int64_t)1 << (3 * bits);
@@ -92,6 +99,22 @@ inline ClusterLayout cluster_layout(int dtype, int64_t natoms, int cap) {
   return L;
 }
 
+// One system of a batch (several independent periodic systems evaluated by the same
+// launches). Clusters, super-clusters, PME grids and box facts of a batch are laid out
+// system after system; every cluster list stays inside its own system.
+struct BatchSys {
+  int64_t atom_off, natoms;    // caller-order atoms in the batch arrays
+  int64_t cl_off, ncl;         // clusters: sorted slots [32 cl_off, 32 (cl_off + ncl))
+  int64_t sup_off, nsup;       // super-clusters
+  int64_t grid_off, cplx_off;  // PME grids: K^3 real points, K*K*(K/2+1) complex points
+  int nc, bits;                // cell grid side and Hilbert bits per axis
+  int K, mod_off;              // PME grid side and offset of its B-spline moduli
+  int pme_blocks, pad;         // blocks of the per-system PME reductions
+};
+
+// Stride of the per-system box facts (see box_info_kernel).
+constexpr int kInfoStride = 32;
+
 // Pointers into one workspace.
 template <class T>
 struct ClusterData {
@@ -105,6 +128,13 @@ struct ClusterData {
   double *boxinfo;  // [0..8] box, [9..17] inv, [18] ortho flag, [19..21] perpendicular widths
   int nc, bits, cap;
   int64_t natoms, nclusters, npad, nsuper;
+  // batch mode: system table and owners (NULL for one system); boxinfo then holds one
+  // record of kInfoStride doubles per system
+  const BatchSys *sys;
+  int *cl_sys;   // owning system of each cluster
+  int *sup_sys;  // owning system of each super-cluster
+  __device__ __forceinline__ int system_of(int64_t cluster) const { return cl_sys ? cl_sys[cluster] : 0; }
+  __device__ __forceinline__ const double *info(int system) const { return boxinfo + kInfoStride * system; }
 };
 
 template <class T>
@@ -137,6 +167,9 @@ inline ClusterData<T> cluster_data(const ClusterLayout &L, void *ws) {
   d.nclusters = L.nclusters;
   d.npad = L.npad;
   d.nsuper = L.nsuper;
+  d.sys = nullptr;
+  d.cl_sys = nullptr;
+  d.sup_sys = nullptr;
   return d;
 }
 
@@ -178,8 +211,7 @@ __device__ __forceinline__ unsigned hilbert_key(unsigned x0, unsigned x1, unsign
 
 // Box facts used by the cluster search: inverse, orthorhombic flag, perpendicular widths.
 template <class T>
-__global__ void box_info_kernel(const T *box, double *info) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ void write_box_info(const T *box, double *info) {
   Box b;
   load_box(box, b);
   for (int k = 0; k < 9; ++k) {
@@ -196,6 +228,11 @@ __global__ void box_info_kernel(const T *box, double *info) {
     double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2], cz = u[0] * v[1] - u[1] * v[0];
     info[19 + d] = b.vol / sqrt(cx * cx + cy * cy + cz * cz);
   }
+}
+
+template <class T>
+__global__ void box_info_kernel(const T *box, double *info) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) write_box_info(box, info);
 }
 
 template <class T>
@@ -319,6 +356,144 @@ __global__ void sort_buckets_kernel(const T *x, const T *q, int64_t nkeys, Clust
   }
 }
 
+// Batch mode, steps 1-5 in one launch: one block per system bins its atoms on the
+// system's own Hilbert-ordered cell grid in shared memory (counting sort, then an
+// insertion sort of each bucket by atom index, which makes the order deterministic and
+// equal to the single-system sort), writes the sorted SoA with padding to whole clusters
+// and the cluster / super-cluster owners. Limits: kBatchMaxAtoms atoms and
+// kBatchMaxKeys keys per system (16 cells per side).
+constexpr int kBatchSortThreads = 1024;
+constexpr int kBatchMaxAtoms = 16384;
+constexpr int kBatchMaxKeys = 4096;
+constexpr size_t kBatchSortSmem = (2 * kBatchMaxKeys + 1) * sizeof(unsigned) + 2 * kBatchMaxAtoms * sizeof(unsigned short);
+
+template <class T>
+__global__ void __launch_bounds__(kBatchSortThreads) batch_sort_kernel(const T *x, const T *q, const T *boxes, int nsys,
+                                                                       ClusterData<T> d) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned *hist = reinterpret_cast<unsigned *>(smem);          // kBatchMaxKeys + 1
+  unsigned *fill = hist + kBatchMaxKeys + 1;                     // kBatchMaxKeys
+  unsigned short *lkey = reinterpret_cast<unsigned short *>(fill + kBatchMaxKeys);  // atom -> key
+  unsigned short *order = lkey + kBatchMaxAtoms;                 // sorted position -> atom
+  __shared__ double s_info[kInfoStride];
+  __shared__ unsigned s_warp[32];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int sy = blockIdx.x; sy < nsys; sy += gridDim.x) {
+    const BatchSys b = d.sys[sy];
+    const int n = (int)b.natoms;
+    const int nkeys = 1 << (3 * b.bits);
+    const T *xs = x + 3 * b.atom_off;
+    if (tid == 0) {
+      write_box_info(boxes + 9 * (int64_t)sy, s_info);
+      for (int k = 0; k < kInfoStride; ++k) d.boxinfo[(int64_t)kInfoStride * sy + k] = s_info[k];
+    }
+    for (int k = tid; k <= nkeys; k += blockDim.x) hist[k] = 0u;
+    for (int k = tid; k < nkeys; k += blockDim.x) fill[k] = 0u;
+    __syncthreads();
+    const double *inv = s_info + 9;
+    for (int t = tid; t < n; t += blockDim.x) {
+      const double rx = xs[3 * t], ry = xs[3 * t + 1], rz = xs[3 * t + 2];
+      unsigned cell[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double v = rx * inv[c] + ry * inv[3 + c] + rz * inv[6 + c];
+        v -= floor(v);
+        if (v >= 1.0) v = 0.0;
+        cell[c] = min((unsigned)(v * b.nc), (unsigned)(b.nc - 1));
+      }
+      const unsigned key = hilbert_key(cell[0], cell[1], cell[2], b.bits);
+      lkey[t] = (unsigned short)key;
+      atomicAdd(&hist[key], 1u);
+    }
+    __syncthreads();
+    // exclusive scan of hist[0, nkeys): thread t owns kBatchMaxKeys / blockDim.x entries
+    {
+      const int per = (nkeys + blockDim.x - 1) / blockDim.x;
+      const int beg = min(tid * per, nkeys), end = min(beg + per, nkeys);
+      unsigned sum = 0u;
+      for (int k = beg; k < end; ++k) sum += hist[k];
+      unsigned incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) s_warp[w] = incl;
+      __syncthreads();
+      if (w == 0) {
+        const unsigned v = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0u;
+        unsigned vi = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned y = __shfl_up_sync(kFull, vi, o);
+          if (lane >= o) vi += y;
+        }
+        s_warp[lane] = vi - v;
+      }
+      __syncthreads();
+      unsigned run = s_warp[w] + incl - sum;
+      for (int k = beg; k < end; ++k) {
+        const unsigned v = hist[k];
+        hist[k] = run;
+        run += v;
+      }
+      if (tid == 0) hist[nkeys] = (unsigned)n;
+    }
+    __syncthreads();
+    for (int t = tid; t < n; t += blockDim.x) {
+      const unsigned key = lkey[t];
+      order[hist[key] + atomicAdd(&fill[key], 1u)] = (unsigned short)t;
+    }
+    __syncthreads();
+    for (int k = tid; k < nkeys; k += blockDim.x) {
+      const int b0 = (int)hist[k], b1 = (int)hist[k + 1];
+      for (int i = b0 + 1; i < b1; ++i) {
+        const unsigned short v = order[i];
+        int j = i - 1;
+        while (j >= b0 && order[j] > v) {
+          order[j + 1] = order[j];
+          --j;
+        }
+        order[j + 1] = v;
+      }
+    }
+    __syncthreads();
+    const double *m = s_info;
+    const int64_t base = b.cl_off * kWarp;
+    const int npad = (int)(b.ncl * kWarp);
+    for (int p = tid; p < npad; p += blockDim.x) {
+      const int64_t slot = base + p;
+      if (p < n) {
+        const int t = order[p];
+        const int64_t a = b.atom_off + t;
+        const double rx = xs[3 * t], ry = xs[3 * t + 1], rz = xs[3 * t + 2];
+        double f[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          double v = rx * inv[c] + ry * inv[3 + c] + rz * inv[6 + c];
+          v -= floor(v);
+          if (v >= 1.0) v = 0.0;
+          f[c] = v;
+        }
+        const double wx = f[0] * m[0] + f[1] * m[3] + f[2] * m[6];
+        const double wy = f[0] * m[1] + f[1] * m[4] + f[2] * m[7];
+        const double wz = f[0] * m[2] + f[1] * m[5] + f[2] * m[8];
+        d.pos[slot] = make_v4((T)wx, (T)wy, (T)wz, q ? q[a] : T(0));
+        d.frac[slot] = make_v4((T)f[0], (T)f[1], (T)f[2], T(0));
+        d.sidx[slot] = (int)a;
+        d.inv[a] = (int)slot;
+      } else {
+        d.sidx[slot] = -1;
+        d.pos[slot] = make_v4(T(0), T(0), T(0), T(0));
+        d.frac[slot] = make_v4(T(0), T(0), T(0), T(0));
+      }
+    }
+    for (int c = tid; c < b.ncl; c += blockDim.x) d.cl_sys[b.cl_off + c] = sy;
+    for (int c = tid; c < b.nsup; c += blockDim.x) d.sup_sys[b.sup_off + c] = sy;
+    __syncthreads();
+  }
+}
+
 // One warp per cluster: bounding box in fractional coordinates. The box is taken around
 // the first atom's image so that a cluster straddling the periodic boundary stays compact,
 // and the cluster's positions are rewritten as that same contiguous image (anchor +
@@ -330,10 +505,19 @@ template <class T>
 __global__ void __launch_bounds__(kWarp * kSuper) cluster_bounds_kernel(ClusterData<T> d) {
   __shared__ double s_box[kSuper][6];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const double *m = d.boxinfo;
   for (int64_t S = blockIdx.x; S < d.nsuper; S += gridDim.x) {
-    const int64_t c = S * kSuper + w;
-    if (c < d.nclusters) {
+    // members [first, last) of super-cluster S, all in one system
+    int64_t first = S * kSuper, last = min(first + kSuper, d.nclusters);
+    int sy = 0;
+    if (d.sys) {
+      sy = d.sup_sys[S];
+      const BatchSys &b = d.sys[sy];
+      first = b.cl_off + (S - b.sup_off) * kSuper;
+      last = min(first + kSuper, b.cl_off + b.ncl);
+    }
+    const double *m = d.info(sy);
+    const int64_t c = first + w;
+    if (c < last) {
       const int64_t s = c * kWarp + lane;
       const bool valid = d.sidx[s] >= 0;
       auto f = d.frac[s];
@@ -371,7 +555,7 @@ __global__ void __launch_bounds__(kWarp * kSuper) cluster_bounds_kernel(ClusterD
     }
     __syncthreads();
     if (w == 0) {
-      const bool v = S * kSuper + lane < d.nclusters;
+      const bool v = first + lane < last;
       double lo[3], hi[3];
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
@@ -433,20 +617,31 @@ __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) 
     const auto ci = d.bc[I];
     const auto hi = d.bh[I];
     int count = 0;
-    const int64_t jend = half ? (I + 1) : d.nclusters;
-    const int64_t send = (jend + kSuper - 1) / kSuper;
+    // candidates: clusters [j0, jend) and super-clusters [s0, send) of I's system
+    int64_t j0 = 0, j1 = d.nclusters, s0 = 0;
+    int sy = 0;
+    if (d.sys) {
+      sy = d.cl_sys[I];
+      const BatchSys &b = d.sys[sy];
+      j0 = b.cl_off;
+      j1 = b.cl_off + b.ncl;
+      s0 = b.sup_off;
+    }
+    const double *info = d.info(sy);
+    const int64_t jend = half ? (I + 1) : j1;
+    const int64_t send = s0 + (jend - j0 + kSuper - 1) / kSuper;
     // Lanes screen 32 super-clusters at a time; the members of each survivor (one per lane,
     // kSuper == kWarp) are then tested in ascending order, so the list is sorted by J.
-    for (int64_t sb = 0; sb < send; sb += kWarp) {
+    for (int64_t sb = s0; sb < send; sb += kWarp) {
       const int64_t S = sb + lane;
-      const bool sok = S < send && clusters_may_interact<T>(ci, hi, d.sbc[S], d.sbh[S], d.boxinfo, rc);
+      const bool sok = S < send && clusters_may_interact<T>(ci, hi, d.sbc[S], d.sbh[S], info, rc);
       unsigned sm = __ballot_sync(kFull, sok);
       while (sm) {
         const int k = __ffs(sm) - 1;
         sm &= sm - 1u;
-        const int64_t J = (sb + k) * kSuper + lane;
+        const int64_t J = j0 + (sb + k - s0) * kSuper + lane;
         bool ok = false;
-        if (J < jend) ok = clusters_may_interact<T>(ci, hi, d.bc[J], d.bh[J], d.boxinfo, rc);
+        if (J < jend) ok = clusters_may_interact<T>(ci, hi, d.bc[J], d.bh[J], info, rc);
         const unsigned mm = __ballot_sync(kFull, ok);
         if (ok) {
           const int r = count + __popc(mm & ((1u << lane) - 1u));

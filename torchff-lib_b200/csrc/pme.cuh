@@ -94,19 +94,17 @@ struct SortedAtoms {
 
 // Spread: a group of kLanesPerAtom lanes per atom; lane g of the group takes the stencil
 // rows r = g, g + kLanesPerAtom, ... of the 36 (x, y) rows, 6 z points each. Loops run at
-// warp granularity so that every lane of a warp takes the same trip count.
+// warp granularity so that every lane of a warp takes the same trip count. `bid` and
+// `nblk` are the block index and count over which the atoms are distributed.
 constexpr int kLanesPerAtom = 8;
 constexpr int kAtomsPerWarp = kWarp / kLanesPerAtom;
 
 template <class T, class Atoms>
-__global__ void __launch_bounds__(kPmeBlock) pme_spread_kernel(Atoms atoms, int64_t nthreads, const T *box, int K,
-                                                               typename Acc<T>::S *grid) {
-  __shared__ PmeShared sh;
-  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
-  __syncthreads();
+__device__ __forceinline__ void spread_atoms(const Atoms &atoms, int64_t nthreads, const PmeShared &sh, int K,
+                                             typename Acc<T>::S *grid, int64_t bid, int64_t nblk) {
   const int g = threadIdx.x % kLanesPerAtom;
-  const int64_t wglob = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
-  const int64_t nwarps = (int64_t)gridDim.x * blockDim.x / kWarp;
+  const int64_t wglob = (bid * blockDim.x + threadIdx.x) / kWarp;
+  const int64_t nwarps = nblk * blockDim.x / kWarp;
   for (int64_t wb = wglob * kAtomsPerWarp; wb < nthreads; wb += nwarps * kAtomsPerWarp) {
     const int64_t t = wb + (threadIdx.x % kWarp) / kLanesPerAtom;
     double rx, ry, rz;
@@ -131,6 +129,15 @@ __global__ void __launch_bounds__(kPmeBlock) pme_spread_kernel(Atoms atoms, int6
   }
 }
 
+template <class T, class Atoms>
+__global__ void __launch_bounds__(kPmeBlock) pme_spread_kernel(Atoms atoms, int64_t nthreads, const T *box, int K,
+                                                               typename Acc<T>::S *grid) {
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
+  __syncthreads();
+  spread_atoms<T>(atoms, nthreads, sh, K, grid, blockIdx.x, gridDim.x);
+}
+
 static __global__ void pme_fix_to_real_kernel(const unsigned long long *gi, float *gf, int64_t n) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
     gf[k] = (float)from_fix(gi[k]);
@@ -140,21 +147,19 @@ template <class T> struct CplxOf;
 template <> struct CplxOf<float> { using type = cufftComplex; };
 template <> struct CplxOf<double> { using type = cufftDoubleComplex; };
 
+// Convolution of the points bid, bid + nblk, ... (in blocks of blockDim.x); returns this
+// thread's share of sum_k w C(k) |S(k)|^2 / theta(k)^2 (the energy is half of the total).
 template <class T>
-__global__ void __launch_bounds__(kPmeBlock) pme_convolve_kernel(typename CplxOf<T>::type *S, const T *box, int K,
-                                                                 double alpha, const T *xmod, const T *ymod,
-                                                                 const T *zmod, double *partials, unsigned *ticket,
-                                                                 double *e_rec) {
-  __shared__ PmeShared sh;
-  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
-  __syncthreads();
+__device__ __forceinline__ double convolve_points(typename CplxOf<T>::type *S, const PmeShared &sh, int K,
+                                                  double alpha, const T *xmod, const T *ymod, const T *zmod,
+                                                  int64_t bid, int64_t nblk) {
   const int Kz = K / 2 + 1;
   const int64_t total = (int64_t)K * K * Kz;
   const double four_pi_over_v = 4.0 * 3.14159265358979323846 / sh.vol;
   const double two_pi = 2.0 * 3.14159265358979323846;
   const double inv4a2 = 1.0 / (4.0 * alpha * alpha);
   double e = 0.0;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t t = bid * blockDim.x + threadIdx.x; t < total; t += nblk * blockDim.x) {
     const int iz = (int)(t % Kz);
     const int iy = (int)((t / Kz) % K);
     const int ix = (int)(t / ((int64_t)Kz * K));
@@ -179,6 +184,18 @@ __global__ void __launch_bounds__(kPmeBlock) pme_convolve_kernel(typename CplxOf
     v.y = (T)(im * factor);
     S[t] = v;
   }
+  return e;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kPmeBlock) pme_convolve_kernel(typename CplxOf<T>::type *S, const T *box, int K,
+                                                                 double alpha, const T *xmod, const T *ymod,
+                                                                 const T *zmod, double *partials, unsigned *ticket,
+                                                                 double *e_rec) {
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
+  __syncthreads();
+  const double e = convolve_points<T>(S, sh, K, alpha, xmod, ymod, zmod, blockIdx.x, gridDim.x);
   grid_sum<kPmeBlock>(0.5 * e, partials, ticket, e_rec, false);
 }
 
@@ -198,19 +215,16 @@ struct PlainGatherOut {
 };
 
 // Gather: kLanesPerAtom lanes per atom as in the spread, partial sums reduced with
-// shuffles inside the lane group (FP64 accumulation of the 216 products).
+// shuffles inside the lane group (FP64 accumulation of the 216 products). Returns this
+// thread's share of the self energy -(a/sqrt(pi)) sum q^2.
 template <class T, class Atoms, class Out>
-__global__ void __launch_bounds__(kPmeBlock) pme_gather_kernel(Atoms atoms, int64_t nthreads, const T *box, int K,
-                                                               const T *Phi, double alpha, Out out, double *partials,
-                                                               unsigned *ticket, double *e_self, const double *e_rec,
-                                                               double e_scale, T *energy_out) {
-  __shared__ PmeShared sh;
-  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
-  __syncthreads();
+__device__ __forceinline__ double gather_atoms(const Atoms &atoms, int64_t nthreads, const PmeShared &sh, int K,
+                                               const T *Phi, double alpha, const Out &out, int64_t bid,
+                                               int64_t nblk) {
   const double a_rpi = alpha / 1.7724538509055160273;
   const int g = threadIdx.x % kLanesPerAtom;
-  const int64_t wglob = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
-  const int64_t nwarps = (int64_t)gridDim.x * blockDim.x / kWarp;
+  const int64_t wglob = (bid * blockDim.x + threadIdx.x) / kWarp;
+  const int64_t nwarps = nblk * blockDim.x / kWarp;
   double e = 0.0;
   for (int64_t wb = wglob * kAtomsPerWarp; wb < nthreads; wb += nwarps * kAtomsPerWarp) {
     const int64_t t = wb + (threadIdx.x % kWarp) / kLanesPerAtom;
@@ -260,8 +274,74 @@ __global__ void __launch_bounds__(kPmeBlock) pme_gather_kernel(Atoms atoms, int6
       e -= a_rpi * qd * qd;
     }
   }
+  return e;
+}
+
+template <class T, class Atoms, class Out>
+__global__ void __launch_bounds__(kPmeBlock) pme_gather_kernel(Atoms atoms, int64_t nthreads, const T *box, int K,
+                                                               const T *Phi, double alpha, Out out, double *partials,
+                                                               unsigned *ticket, double *e_self, const double *e_rec,
+                                                               double e_scale, T *energy_out) {
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
+  __syncthreads();
+  const double e = gather_atoms<T>(atoms, nthreads, sh, K, Phi, alpha, out, blockIdx.x, gridDim.x);
   const bool last = grid_sum<kPmeBlock>(e, partials, ticket, e_self, false);
   if (last && threadIdx.x == 0 && energy_out) energy_out[0] = (T)(e_scale * (*e_rec + *e_self));
+}
+
+// ---- batched PME: blockIdx.y is the system, blocks [0, BatchSys::pme_blocks) of it work
+// (a count that depends on the system alone, so that its reductions sum in the same order
+// whatever else is in the batch).
+constexpr int kBatchPmeMaxBlocks = 256;
+
+template <class T>
+__global__ void __launch_bounds__(kPmeBlock) batch_spread_kernel(const BatchSys *sys, const T *x, const T *q,
+                                                                 const T *boxes, typename Acc<T>::S *grid) {
+  const BatchSys &b = sys[blockIdx.y];
+  if (blockIdx.x >= (unsigned)b.pme_blocks) return;
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)blockIdx.y, b.K, sh);
+  __syncthreads();
+  PlainAtoms<T> atoms{x + 3 * b.atom_off, q + b.atom_off, b.natoms};
+  spread_atoms<T>(atoms, b.natoms, sh, b.K, grid + b.grid_off, blockIdx.x, b.pme_blocks);
+}
+
+// partials: kBatchPmeMaxBlocks per system; tickets and energies: 2 per system
+// ([2s] reciprocal, [2s+1] self).
+template <class T>
+__global__ void __launch_bounds__(kPmeBlock) batch_convolve_kernel(const BatchSys *sys, typename CplxOf<T>::type *S,
+                                                                   const T *boxes, double alpha, const T *moduli,
+                                                                   double *partials, unsigned *tickets,
+                                                                   double *energies) {
+  const int sy = blockIdx.y;
+  const BatchSys &b = sys[sy];
+  if (blockIdx.x >= (unsigned)b.pme_blocks) return;
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
+  __syncthreads();
+  const T *xm = moduli + b.mod_off, *ym = xm + b.K, *zm = ym + b.K;
+  const double e = convolve_points<T>(S + b.cplx_off, sh, b.K, alpha, xm, ym, zm, blockIdx.x, b.pme_blocks);
+  grid_sum_n<kPmeBlock>(0.5 * e, partials + (int64_t)kBatchPmeMaxBlocks * sy, tickets + 2 * sy, energies + 2 * sy,
+                        false, blockIdx.x, b.pme_blocks);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kPmeBlock) batch_gather_kernel(const BatchSys *sys, const T *x, const T *q,
+                                                                 const T *boxes, const T *Phi, double alpha, T *phi,
+                                                                 T *grad, double *partials, unsigned *tickets,
+                                                                 double *energies) {
+  const int sy = blockIdx.y;
+  const BatchSys &b = sys[sy];
+  if (blockIdx.x >= (unsigned)b.pme_blocks) return;
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
+  __syncthreads();
+  PlainAtoms<T> atoms{x + 3 * b.atom_off, q + b.atom_off, b.natoms};
+  PlainGatherOut<T> out{phi + b.atom_off, grad + 3 * b.atom_off};
+  const double e = gather_atoms<T>(atoms, b.natoms, sh, b.K, Phi + b.grid_off, alpha, out, blockIdx.x, b.pme_blocks);
+  grid_sum_n<kPmeBlock>(e, partials + (int64_t)kBatchPmeMaxBlocks * sy, tickets + 2 * sy + 1, energies + 2 * sy + 1,
+                        false, blockIdx.x, b.pme_blocks);
 }
 
 // Scratch layout of one PME evaluation.

@@ -159,22 +159,24 @@ __device__ __forceinline__ double block_sum(double v) {
 // into `*out` (replacing it, or adding when `accumulate`). `ticket` must be 0 before the
 // launch and is reset to 0 by the last block, so repeated launches need no memset.
 // Returns true (block-uniform) in the last block, whose thread 0 has written *out.
+// grid_sum_n reduces over the blocks bid = 0 .. nblocks-1 of one group (e.g. the blocks of
+// one system in a batched launch); grid_sum over the whole grid.
 template <int BLOCK>
-__device__ __forceinline__ bool grid_sum(double v, double *partials, unsigned *ticket,
-                                         double *out, bool accumulate) {
+__device__ __forceinline__ bool grid_sum_n(double v, double *partials, unsigned *ticket, double *out,
+                                           bool accumulate, unsigned bid, unsigned nblocks) {
   __shared__ bool s_last;
   double s = block_sum<BLOCK>(v);
   if (threadIdx.x == 0) {
-    partials[blockIdx.x] = s;
+    partials[bid] = s;
     __threadfence();
     unsigned t = atomicAdd(ticket, 1u);
-    s_last = (t == gridDim.x - 1);
+    s_last = (t == nblocks - 1);
   }
   __syncthreads();
   if (s_last) {
     __threadfence();
     double a = 0.0;
-    for (unsigned i = threadIdx.x; i < gridDim.x; i += BLOCK)
+    for (unsigned i = threadIdx.x; i < nblocks; i += BLOCK)
       a += *((volatile double *)partials + i);
     double tot = block_sum<BLOCK>(a);
     if (threadIdx.x == 0) {
@@ -183,6 +185,12 @@ __device__ __forceinline__ bool grid_sum(double v, double *partials, unsigned *t
     }
   }
   return s_last;
+}
+
+template <int BLOCK>
+__device__ __forceinline__ bool grid_sum(double v, double *partials, unsigned *ticket,
+                                         double *out, bool accumulate) {
+  return grid_sum_n<BLOCK>(v, partials, ticket, out, accumulate, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------------

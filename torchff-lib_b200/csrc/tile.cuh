@@ -1,0 +1,478 @@
+// Fused real-space kernels shared by the single-system and the batched evaluation.
+//
+// Tile kernel: one warp per work item = cluster I (lane l owns atom l of I) and up to
+// kItemTiles clusters J taken with a stride from I's FULL neighbour list (entries k,
+// k + n, k + 2n, ... for n = ceil(count / kItemTiles)), so that each item samples
+// neighbours in every direction and the lanes get similar amounts of work.
+//   pass 1: the J clusters are staged in shared memory; every lane sweeps the 32 atoms of
+//           each with broadcast reads and builds a 32-bit in-cutoff mask per tile;
+//   pass 2: each lane walks its own set bits across all tiles of the item and evaluates
+//           LJ + erfc Coulomb only there;
+//   pass 3: excluded pairs inside the cutoff get the Ewald exclusion correction.
+// A cluster pair whose boxes are close enough uses one periodic shift for all its pairs
+// (positions are cluster-contiguous images); other pairs use the per-pair minimum image.
+// Each pair is evaluated from both sides, which removes j-side atomics: forces / charge
+// gradients of atom i are summed in registers and added once per item into int64 fixed
+// point accumulators (mixed) or FP64 atomics (FP64 mode); energies likewise, halved. With
+// no block barrier a warp that finishes early does not wait for its block.
+#pragma once
+
+#include <cmath>
+#include <vector>
+
+#include "pme.cuh"
+
+namespace tff {
+namespace {
+
+constexpr int kMaxExcl = 8;       // excluded partners per atom (self excluded)
+
+// Warps per block of the tile kernel: 4 (FP32) or 2 (FP64) so that the staged tiles fit in
+// 48 KB of static shared memory.
+template <class T> struct TileCfg { static constexpr int NW = sizeof(T) == 8 ? 2 : 4; };
+
+template <class T> struct V2;
+template <> struct V2<float> { using type = float2; };
+struct __align__(16) D2 { double x, y; };
+template <> struct V2<double> { using type = D2; };
+__device__ __forceinline__ float2 make_v2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ D2 make_v2(double a, double b) { return D2{a, b}; }
+
+__device__ __forceinline__ float erf_t(float x) { return erff(x); }
+__device__ __forceinline__ double erf_t(double x) { return erf(x); }
+
+// erfc(u) and exp(-u^2) of the FP64 path (the FP32 path inlines A&S 7.1.26 in pass 2).
+__device__ __forceinline__ void erfc_exp(double u, double &ec, double &ex) {
+  ec = erfc(u);
+  ex = exp(-u * u);
+}
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+
+template <class T>
+struct TileArgs {
+  ClusterData<T> cl;
+  const typename V2<T>::type *lj;  // sorted slots: (sigma/2, sqrt(eps))
+  const int *exslot;               // (npad, kMaxExcl) sorted slots of excluded partners, -1 padded
+  typename Acc<T>::S *gx;          // (npad, 3) sorted slots, dE/dx
+  typename Acc<T>::S *gq;          // (npad) sorted slots, dE/dq
+  double rc, alpha, kc;
+  typename Acc<T>::S *energies;    // per system: [2s] pairs (LJ + erfc Coulomb), [2s+1] exclusion correction
+};
+
+// LB parameters and excluded-partner slots in sorted order. Partner indices are counted
+// from the first atom of the atom's own system (batch mode), i.e. global for one system.
+template <class T>
+__global__ void sorted_params_kernel(ClusterData<T> cl, const T *sigma, const T *eps, const int *excl,
+                                     typename V2<T>::type *lj, int *exslot) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < cl.npad; s += (int64_t)gridDim.x * blockDim.x) {
+    const int a = cl.sidx[s];
+    const int64_t base = (cl.sys && a >= 0) ? cl.sys[cl.cl_sys[s / kWarp]].atom_off : 0;
+    lj[s] = a >= 0 ? make_v2(T(0.5) * sigma[a], (T)sqrt((double)eps[a])) : make_v2(T(0), T(0));
+#pragma unroll
+    for (int k = 0; k < kMaxExcl; ++k) {
+      const int p = a >= 0 ? excl[(int64_t)a * kMaxExcl + k] : -1;
+      exslot[s * kMaxExcl + k] = p >= 0 ? cl.inv[base + p] : -1;
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void pair_min_image(bool ortho, T &dx, T &dy, T &dz, const T *m, const T *inv) {
+  if (ortho) {
+    dx = wrap1(dx, m[0], inv[0]);
+    dy = wrap1(dy, m[4], inv[4]);
+    dz = wrap1(dz, m[8], inv[8]);
+  } else {
+    min_image(dx, dy, dz, m, inv);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(TileCfg<T>::NW * 32) tile_kernel(TileArgs<T> A) {
+  using V = typename V4<T>::type;
+  using W2 = typename V2<T>::type;
+  constexpr int NW = TileCfg<T>::NW;
+  __shared__ V s_pos[NW][kItemTiles][kWarp];
+  __shared__ W2 s_lj[NW][kItemTiles][kWarp];
+  // negated j positions, structure of arrays, for the packed FP32 distance pass
+  __shared__ __align__(8) float s_nx[NW][kItemTiles][sizeof(T) == 4 ? kWarp : 2];
+  __shared__ __align__(8) float s_ny[NW][kItemTiles][sizeof(T) == 4 ? kWarp : 2];
+  __shared__ __align__(8) float s_nz[NW][kItemTiles][sizeof(T) == 4 ? kWarp : 2];
+  __shared__ unsigned s_mask[NW][kItemTiles][kWarp];   // in-cutoff, not excluded
+  __shared__ unsigned s_xmask[NW][kItemTiles][kWarp];  // in-cutoff, excluded
+  __shared__ int s_mi[NW][kItemTiles];                 // 1: tile needs the per-pair minimum image
+  __shared__ T s_box[NW][2][9];                         // box and inverse of the warp's current system
+  const ClusterData<T> &cl = A.cl;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  T *s_m = s_box[w][0], *s_inv = s_box[w][1];
+  int cur_sys = -1;
+  bool ortho = false;
+  const T rc2 = (T)(A.rc * A.rc);
+  const T alpha = (T)A.alpha;
+  const T kc = (T)A.kc;
+  const T two_a_rpi = (T)(2.0 * A.alpha / 1.7724538509055160273);
+
+  const int nitems = cl.itemoff[cl.nclusters];
+  const int nwarps = gridDim.x * NW;
+  for (int it = blockIdx.x * NW + w; it < nitems; it += nwarps) {
+    const int I = cl.items[it];  // owning cluster: itemoff[I] <= it < itemoff[I + 1]
+    const int isys = cl.system_of(I);
+    if (isys != cur_sys) {
+      const double *info = cl.info(isys);
+      if (lane < 9) {
+        s_m[lane] = (T)info[lane];
+        s_inv[lane] = (T)info[9 + lane];
+      }
+      ortho = info[18] != 0.0;
+      cur_sys = isys;
+      __syncwarp();
+    }
+    const int k = it - cl.itemoff[I];
+    const int nch = cl.itemoff[I + 1] - cl.itemoff[I];
+    const int cnt = cl.ncount[I];
+    const int ntile = (cnt - k + nch - 1) / nch;  // this item takes list entries k, k+nch, ...
+    const int64_t si = (int64_t)I * kWarp + lane;
+    const bool vi = cl.sidx[si] >= 0;
+    const V pi = cl.pos[si];
+    const W2 lji = A.lj[si];
+    const T kqi = kc * pi.w;
+    const V ci = cl.bc[I], hi_ = cl.bh[I];
+
+    // stage the tiles and build their cutoff masks (pass 1)
+    for (int t = 0; t < ntile; ++t) {
+      const int J = cl.nbr[(int64_t)I * cl.cap + k + t * nch];
+      const int64_t sj = (int64_t)J * kWarp + lane;
+      // one periodic shift for the whole cluster pair when every pair's displacement then
+      // lies within half a box length per axis (orthorhombic boxes)
+      bool shifted = false;
+      T sx = T(0), sy = T(0), sz = T(0);
+      if (ortho) {
+        const V cj = cl.bc[J], hj = cl.bh[J];
+        const T dcx = ci.x - cj.x, dcy = ci.y - cj.y, dcz = ci.z - cj.z;
+        const T nx = floor(dcx + T(0.5)), ny = floor(dcy + T(0.5)), nz = floor(dcz + T(0.5));
+        shifted = (fabs(dcx - nx) + hi_.x + hj.x < T(0.49)) && (fabs(dcy - ny) + hi_.y + hj.y < T(0.49)) &&
+                  (fabs(dcz - nz) + hi_.z + hj.z < T(0.49));
+        sx = nx * s_m[0];
+        sy = ny * s_m[4];
+        sz = nz * s_m[8];
+      }
+      V pj = cl.pos[sj];
+      if (shifted) {
+        pj.x += sx;
+        pj.y += sy;
+        pj.z += sz;
+      }
+      s_pos[w][t][lane] = pj;
+      s_lj[w][t][lane] = A.lj[sj];
+      if (sizeof(T) == 4) {
+        s_nx[w][t][lane] = -(float)pj.x;
+        s_ny[w][t][lane] = -(float)pj.y;
+        s_nz[w][t][lane] = -(float)pj.z;
+      }
+      const unsigned jvalid = __ballot_sync(kFull, cl.sidx[sj] >= 0);
+      __syncwarp();
+      unsigned mask = 0u;
+      if (sizeof(T) == 4 && shifted) {
+        // two j atoms per step with paired FP32 instructions (FADD2/FMUL2/FFMA2)
+        const float2 px = make_float2((float)pi.x, (float)pi.x), py = make_float2((float)pi.y, (float)pi.y),
+                     pz = make_float2((float)pi.z, (float)pi.z);
+        const float rc2f = (float)rc2;
+#pragma unroll 4
+        for (int s = 0; s < kWarp; s += 2) {
+          const float2 nx = *reinterpret_cast<const float2 *>(&s_nx[w][t][s]);
+          const float2 ny = *reinterpret_cast<const float2 *>(&s_ny[w][t][s]);
+          const float2 nz = *reinterpret_cast<const float2 *>(&s_nz[w][t][s]);
+          const float2 dx = __fadd2_rn(px, nx), dy = __fadd2_rn(py, ny), dz = __fadd2_rn(pz, nz);
+          float2 r2 = __fmul2_rn(dx, dx);
+          r2 = __ffma2_rn(dy, dy, r2);
+          r2 = __ffma2_rn(dz, dz, r2);
+          mask |= (r2.x <= rc2f ? 1u : 0u) << s;
+          mask |= (r2.y <= rc2f ? 2u : 0u) << s;
+        }
+      } else {
+#pragma unroll 8
+        for (int s = 0; s < kWarp; ++s) {
+          const V q = s_pos[w][t][s];
+          T dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+          if (!shifted) pair_min_image(ortho, dx, dy, dz, s_m, s_inv);
+          const T r2 = dx * dx + dy * dy + dz * dz;
+          mask |= (r2 <= rc2) ? (1u << s) : 0u;
+        }
+      }
+      mask &= jvalid;
+      if (J == I) mask &= ~(1u << lane);
+      if (!vi) mask = 0u;
+      unsigned emask = 0u;
+      if (mask) {
+#pragma unroll
+        for (int x = 0; x < kMaxExcl; ++x) {
+          const int xs = A.exslot[si * kMaxExcl + x];
+          if (xs >= 0 && (xs >> 5) == J) emask |= 1u << (xs & 31);
+        }
+      }
+      s_mask[w][t][lane] = mask & ~emask;
+      s_xmask[w][t][lane] = mask & emask;
+      if (lane == 0) s_mi[w][t] = !shifted;
+    }
+    __syncwarp();
+
+    // pass 2: every lane walks its own in-cutoff pairs across all tiles of the item
+    T fx = T(0), fy = T(0), fz = T(0), dq = T(0);
+    double ep = 0.0;
+    if constexpr (sizeof(T) == 4) {
+      // FP32: two pairs per iteration with paired instructions (FADD2/FMUL2/FFMA2); only
+      // rsqrt, reciprocal and exp2 stay scalar. A lane with an odd count pads the second
+      // slot with a zero-charge, zero-epsilon copy of the first, which contributes nothing.
+      const float2 one2 = make_float2(1.f, 1.f), mone2 = make_float2(-1.f, -1.f);
+      const float2 al2 = make_float2(alpha, alpha), ta2 = make_float2(two_a_rpi, two_a_rpi);
+      const float2 nkq2 = make_float2(-kqi, -kqi), kq2 = make_float2(kqi, kqi);
+      const float2 pix = make_float2(pi.x, pi.x), piy = make_float2(pi.y, pi.y), piz = make_float2(pi.z, pi.z);
+      const float2 sgi = make_float2(lji.x, lji.x), epi = make_float2(lji.y, lji.y);
+      float2 fx2 = make_float2(0.f, 0.f), fy2 = fx2, fz2 = fx2, dq2 = fx2, te2 = fx2;
+      int t = 0, iter = 0;
+      unsigned m = ntile > 0 ? s_mask[w][0][lane] : 0u;
+      while (true) {
+        int ta = 0, sa = 0, tb = 0, sb = 0;
+        while (m == 0u && ++t < ntile) m = s_mask[w][t][lane];
+        const bool ha = m != 0u;
+        if (ha) {
+          sa = __ffs(m) - 1;
+          m &= m - 1u;
+          ta = t;
+        }
+        while (m == 0u && ++t < ntile) m = s_mask[w][t][lane];
+        const bool hb = m != 0u;
+        if (hb) {
+          sb = __ffs(m) - 1;
+          m &= m - 1u;
+          tb = t;
+        }
+        if (!__any_sync(kFull, ha)) break;
+        if ((++iter & 15) == 0) {
+          ep += (double)(te2.x + te2.y);
+          te2 = make_float2(0.f, 0.f);
+        }
+        if (ha) {
+          const float4 qa = s_pos[w][ta][sa];
+          float4 qb = hb ? s_pos[w][tb][sb] : make_float4(qa.x, qa.y, qa.z, 0.f);
+          const float2 la = s_lj[w][ta][sa];
+          const float2 lb = hb ? s_lj[w][tb][sb] : make_float2(0.f, 0.f);
+          float2 dx = __fadd2_rn(pix, make_float2(-qa.x, -qb.x));
+          float2 dy = __fadd2_rn(piy, make_float2(-qa.y, -qb.y));
+          float2 dz = __fadd2_rn(piz, make_float2(-qa.z, -qb.z));
+          if (s_mi[w][ta]) pair_min_image(ortho, dx.x, dy.x, dz.x, s_m, s_inv);
+          if (hb && s_mi[w][tb]) pair_min_image(ortho, dx.y, dy.y, dz.y, s_m, s_inv);
+          float2 r2 = __fmul2_rn(dx, dx);
+          r2 = __ffma2_rn(dy, dy, r2);
+          r2 = __ffma2_rn(dz, dz, r2);
+          const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+          const float2 rinv2 = __fmul2_rn(rinv, rinv);
+          const float2 u = __fmul2_rn(__fmul2_rn(r2, rinv), al2);
+          // erfc(u) exp(u^2) by Abramowitz & Stegun 7.1.26 (see erfc_exp_as)
+          const float2 den = __ffma2_rn(u, make_float2(0.3275911f, 0.3275911f), one2);
+          const float2 tt = make_float2(__fdividef(1.f, den.x), __fdividef(1.f, den.y));
+          float2 poly = __ffma2_rn(tt, make_float2(1.061405429f, 1.061405429f),
+                                   make_float2(-1.453152027f, -1.453152027f));
+          poly = __ffma2_rn(tt, poly, make_float2(1.421413741f, 1.421413741f));
+          poly = __ffma2_rn(tt, poly, make_float2(-0.284496736f, -0.284496736f));
+          poly = __ffma2_rn(tt, poly, make_float2(0.254829592f, 0.254829592f));
+          poly = __fmul2_rn(tt, poly);
+          const float2 mu2 = __fmul2_rn(u, u);
+          const float2 ex = make_float2(__expf(-mu2.x), __expf(-mu2.y));
+          const float2 ec = __fmul2_rn(poly, ex);
+          const float2 qj = make_float2(qa.w, qb.w);
+          const float2 cq = __fmul2_rn(__fmul2_rn(qj, ec), rinv);  // E_coul / (k q_i)
+          const float2 g = __ffma2_rn(ta2, __fmul2_rn(ex, rinv), __fmul2_rn(ec, rinv2));
+          float2 dedr = __fmul2_rn(__fmul2_rn(g, rinv), __fmul2_rn(qj, nkq2));
+          const float2 sig = __fadd2_rn(sgi, make_float2(la.x, lb.x));
+          const float2 eps = __fmul2_rn(epi, make_float2(la.y, lb.y));
+          const float2 sr2 = __fmul2_rn(__fmul2_rn(sig, sig), rinv2);
+          const float2 sr6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
+          const float2 es6 = __fmul2_rn(eps, sr6);
+          dedr = __ffma2_rn(__fmul2_rn(es6, make_float2(-24.f, -24.f)),
+                            __fmul2_rn(__ffma2_rn(sr6, make_float2(2.f, 2.f), mone2), rinv2), dedr);
+          fx2 = __ffma2_rn(dedr, dx, fx2);
+          fy2 = __ffma2_rn(dedr, dy, fy2);
+          fz2 = __ffma2_rn(dedr, dz, fz2);
+          dq2 = __fadd2_rn(dq2, cq);
+          te2 = __ffma2_rn(cq, kq2, te2);
+          te2 = __ffma2_rn(__fmul2_rn(es6, make_float2(4.f, 4.f)), __fadd2_rn(sr6, mone2), te2);
+        }
+      }
+      ep += (double)(te2.x + te2.y);
+      fx = fx2.x + fx2.y;
+      fy = fy2.x + fy2.y;
+      fz = fz2.x + fz2.y;
+      dq = dq2.x + dq2.y;
+    } else {
+      T te = T(0);  // partial energy, moved into ep every 16 pairs
+      int t = 0, iter = 0;
+      unsigned m = ntile > 0 ? s_mask[w][0][lane] : 0u;
+      while (true) {
+        while (m == 0u && ++t < ntile) m = s_mask[w][t][lane];
+        const bool have = m != 0u;
+        if (!__any_sync(kFull, have)) break;
+        if ((++iter & 15) == 0) {
+          ep += (double)te;
+          te = T(0);
+        }
+        if (have) {
+          const int s = __ffs(m) - 1;
+          m &= m - 1u;
+          const V q = s_pos[w][t][s];
+          const W2 ljj = s_lj[w][t][s];
+          T dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+          if (s_mi[w][t]) pair_min_image(ortho, dx, dy, dz, s_m, s_inv);
+          const T r2 = dx * dx + dy * dy + dz * dz;
+          const T rinv = rsqrt_t(r2);
+          const T rinv2 = rinv * rinv;
+          const T u = alpha * (r2 * rinv);
+          T ec, ex2;
+          erfc_exp(u, ec, ex2);
+          const T cq = q.w * ec * rinv;  // E_coul / (k q_i)
+          T dedr_r = -kqi * q.w * (ec * rinv2 + two_a_rpi * ex2 * rinv) * rinv;
+          const T sig = lji.x + ljj.x;
+          const T eps = lji.y * ljj.y;
+          const T sr2 = sig * sig * rinv2;
+          const T sr6 = sr2 * sr2 * sr2;
+          dedr_r -= T(24) * eps * sr6 * (T(2) * sr6 - T(1)) * rinv2;
+          fx += dedr_r * dx;
+          fy += dedr_r * dy;
+          fz += dedr_r * dz;
+          dq += cq;
+          te += kqi * cq + T(4) * eps * sr6 * (sr6 - T(1));
+        }
+      }
+      ep += (double)te;
+    }
+    // pass 3: excluded pairs within the cutoff: Ewald exclusion correction
+    // k q_i q_j (erfc(u) - 1)/r = -k q_i q_j erf(u)/r, no LJ
+    double ex = 0.0;
+    int t = 0;
+    unsigned m = ntile > 0 ? s_xmask[w][0][lane] : 0u;
+    while (true) {
+      while (m == 0u && ++t < ntile) m = s_xmask[w][t][lane];
+      const bool have = m != 0u;
+      if (!__any_sync(kFull, have)) break;
+      if (have) {
+        const int s = __ffs(m) - 1;
+        m &= m - 1u;
+        const V q = s_pos[w][t][s];
+        T dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+        if (s_mi[w][t]) pair_min_image(ortho, dx, dy, dz, s_m, s_inv);
+        const T r2 = dx * dx + dy * dy + dz * dz;
+        const T rinv = rsqrt_t(r2);
+        const T u = alpha * (r2 * rinv);
+        const T damp = -erf_t(u);
+        const T ex2 = exp(-u * u);
+        const T cq = q.w * damp * rinv;
+        const T dedr_r = -kqi * q.w * (damp * rinv * rinv + two_a_rpi * ex2 * rinv) * rinv;
+        fx += dedr_r * dx;
+        fy += dedr_r * dy;
+        fz += dedr_r * dz;
+        dq += cq;
+        ex += (double)(kqi * cq);
+      }
+    }
+    if (vi) {
+      Acc<T>::add(&A.gx[3 * si], (double)fx);
+      Acc<T>::add(&A.gx[3 * si + 1], (double)fy);
+      Acc<T>::add(&A.gx[3 * si + 2], (double)fz);
+      Acc<T>::add(&A.gq[si], (double)kc * (double)dq);
+    }
+    // energies: warp sum, then one order-independent accumulation per work item
+    ep = warp_sum(ep);
+    ex = warp_sum(ex);
+    if (lane == 0) {
+      Acc<T>::add(&A.energies[2 * isys], 0.5 * ep);
+      Acc<T>::add(&A.energies[2 * isys + 1], 0.5 * ex);
+    }
+    __syncwarp();
+  }
+}
+
+// Sorted real-space accumulators + caller-order PME derivatives -> caller order; energies
+// of each of the nsys systems (e_tile_acc and e_pme hold two values per system, terms
+// gets four: real-space pairs, exclusion correction, reciprocal, self).
+template <class T>
+__global__ void finalize_kernel(ClusterData<T> cl, const typename Acc<T>::S *gx, const typename Acc<T>::S *gq,
+                                const T *pme_grad, const T *pme_phi, T *forces, double *forces64, T *grad_q,
+                                const typename Acc<T>::S *e_tile_acc, const double *e_pme, double kc,
+                                double *energy, double *terms, int nsys) {
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < cl.natoms;
+       a += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = cl.inv[a];
+    double x = Acc<T>::get(&gx[3 * s]), y = Acc<T>::get(&gx[3 * s + 1]), z = Acc<T>::get(&gx[3 * s + 2]);
+    double g = Acc<T>::get(&gq[s]);
+    if (pme_grad) {
+      x += kc * (double)pme_grad[3 * a];
+      y += kc * (double)pme_grad[3 * a + 1];
+      z += kc * (double)pme_grad[3 * a + 2];
+      g += kc * (double)pme_phi[a];
+    }
+    if (forces) {
+      forces[3 * a] = (T)(-x);
+      forces[3 * a + 1] = (T)(-y);
+      forces[3 * a + 2] = (T)(-z);
+    }
+    if (forces64) {
+      forces64[3 * a] = -x;
+      forces64[3 * a + 1] = -y;
+      forces64[3 * a + 2] = -z;
+    }
+    if (grad_q) grad_q[a] = (T)g;
+  }
+  for (int sy = blockIdx.x * blockDim.x + threadIdx.x; sy < nsys; sy += gridDim.x * blockDim.x) {
+    const double e_tile[2] = {Acc<T>::get(&e_tile_acc[2 * sy]), Acc<T>::get(&e_tile_acc[2 * sy + 1])};
+    const double rec = e_pme ? kc * e_pme[2 * sy] : 0.0;
+    const double self = e_pme ? kc * e_pme[2 * sy + 1] : 0.0;
+    const double tot = e_tile[0] + e_tile[1] + rec + self;
+    if (energy) energy[sy] = tot;
+    if (terms) {
+      terms[4 * sy] = e_tile[0];
+      terms[4 * sy + 1] = e_tile[1];
+      terms[4 * sy + 2] = rec;
+      terms[4 * sy + 3] = self;
+    }
+  }
+}
+
+template <class T>
+__global__ void cast_inputs_kernel(const double *x64, const double *box64, T *x, T *box, int64_t n3) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += (int64_t)gridDim.x * blockDim.x)
+    x[k] = (T)x64[k];
+  if (blockIdx.x == 0 && threadIdx.x < 9) box[threadIdx.x] = (T)box64[threadIdx.x];
+}
+
+// Host-side B-spline moduli theta(k) = sum_{m=-3}^{2} M6(m+3) cos(2 pi m k / K)
+// (torchff/bsplines.py:20-63), with M6 at the integers from the same recursion as the
+// device splines.
+inline void host_bspline6_at_integers(double val[6]) {
+  double m[6] = {0, 1, 0, 0, 0, 0};  // M2(0)=0, M2(1)=1
+  for (int n = 3; n <= 6; ++n) {
+    double nm[6] = {0};
+    for (int k = 0; k < n; ++k) {
+      const double cur = (k < n - 1) ? m[k] : 0.0;
+      const double prev = (k > 0) ? m[k - 1] : 0.0;
+      nm[k] = ((double)k * cur + (double)(n - k) * prev) / (double)(n - 1);
+    }
+    for (int k = 0; k < 6; ++k) m[k] = nm[k];
+  }
+  for (int k = 0; k < 6; ++k) val[k] = m[k];
+}
+
+inline std::vector<double> host_moduli(int K, int count) {
+  double b[6];
+  host_bspline6_at_integers(b);
+  std::vector<double> out(count);
+  for (int k = 0; k < count; ++k) {
+    double s = 0.0;
+    for (int m = -3; m < 3; ++m) s += b[m + 3] * std::cos(2.0 * M_PI * m * k / K);
+    out[k] = s;
+  }
+  return out;
+}
+
+}  // namespace
+}  // namespace tff

@@ -14,6 +14,7 @@ from .nonbonded import (Nonbonded, compute_nonbonded_energy_from_atom_pairs,
                         compute_nonbonded_forces_from_atom_pairs)
 from .pbc import PBC, applyPBC
 from .pme import PME
+from .serving import BatchEvaluator, Server, SystemSpec, autotune_atoms_per_cell
 from .system import FixedChargeNonbonded, FixedChargeSystem
 from .vdw import Vdw, compute_lennard_jones_energy
 
@@ -22,4 +23,5 @@ __all__ = [
     "NeighborList", "build_neighbor_list_cell_list", "build_neighbor_list_nsquared", "Nonbonded",
     "compute_nonbonded_energy_from_atom_pairs", "compute_nonbonded_forces_from_atom_pairs", "PBC", "applyPBC",
     "PME", "FixedChargeNonbonded", "FixedChargeSystem", "Vdw", "compute_lennard_jones_energy",
+    "BatchEvaluator", "Server", "SystemSpec", "autotune_atoms_per_cell",
 ]

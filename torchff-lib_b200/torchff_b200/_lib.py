@@ -14,8 +14,9 @@ from ._build import lib_path
 
 TFF_F32, TFF_F64 = 0, 1
 TFF_OK = 0
+TFF_ERR_TIMEOUT = 6
 _STATUS = {1: "invalid argument", 2: "CUDA error", 3: "cuFFT error", 4: "workspace too small",
-           5: "capacity overflow"}
+           5: "capacity overflow", 6: "timeout"}
 
 _path = lib_path()
 if not os.path.exists(_path):
@@ -30,6 +31,30 @@ class SystemDesc(C.Structure):
     _fields_ = [("dtype", C.c_int), ("natoms", C.c_int64), ("cutoff", C.c_double),
                 ("ewald_alpha", C.c_double), ("pme_grid", C.c_int), ("coul_constant", C.c_double),
                 ("max_cluster_neighbors", C.c_int)]
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [("dtype", C.c_int), ("max_systems", C.c_int), ("max_atoms", C.c_int64),
+                ("max_grid_points", C.c_int64), ("cutoff", C.c_double), ("ewald_alpha", C.c_double),
+                ("coul_constant", C.c_double), ("max_cluster_neighbors", C.c_int), ("atoms_per_cell", C.c_double)]
+
+
+class ServerDesc(C.Structure):
+    _fields_ = [("dtype", C.c_int), ("lanes", C.c_int), ("max_systems_per_batch", C.c_int),
+                ("hbm_budget_bytes", C.c_size_t), ("grid_points_per_atom", C.c_double), ("cutoff", C.c_double),
+                ("ewald_alpha", C.c_double), ("coul_constant", C.c_double), ("atoms_per_cell", C.c_double)]
+
+
+class RequestDesc(C.Structure):
+    _fields_ = [("natoms", C.c_int64), ("pme_grid", C.c_int), ("coords", C.c_void_p), ("box", C.c_void_p),
+                ("charges", C.c_void_p), ("sigma", C.c_void_p), ("epsilon", C.c_void_p), ("nexcl", C.c_int64),
+                ("excl_pairs", C.c_void_p), ("energy", C.c_void_p), ("forces", C.c_void_p)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(name, C.c_int64) for name in (
+        "submitted", "systems_launched", "systems_done", "batches", "max_batch_systems", "max_batch_atoms",
+        "max_lanes_in_flight", "lane_max_atoms", "lane_max_grid_points", "lane_device_bytes")] + [("now", C.c_double)]
 
 
 _SIGS = {
@@ -65,6 +90,21 @@ _SIGS = {
     "tff_timer_elapsed_ms": (i32, [vp, i32, i32, C.POINTER(C.c_float)]),
     "tff_system_eval_timed": (i32, [vp, vp, vp, vp, vp, vp, vp]),
     "tff_system_kernel_launches": (i32, [vp]),
+    "tff_batch_device_bytes": (sz, [C.POINTER(BatchDesc)]),
+    "tff_batch_create": (i32, [C.POINTER(BatchDesc), C.POINTER(vp)]),
+    "tff_batch_destroy": (i32, [vp]),
+    "tff_batch_eval": (i32, [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "tff_batch_status": (i32, [vp, vp, C.POINTER(C.c_int)]),
+    "tff_batch_kernel_launches": (i32, [vp]),
+    "tff_server_create": (i32, [C.POINTER(ServerDesc), C.POINTER(vp)]),
+    "tff_server_destroy": (i32, [vp]),
+    "tff_server_submit": (i32, [vp, C.POINTER(RequestDesc), C.POINTER(i64)]),
+    "tff_server_wait": (i32, [vp, i64, f64]),
+    "tff_server_poll": (i32, [vp, i64, C.POINTER(C.c_int)]),
+    "tff_server_request_times": (i32, [vp, i64, C.POINTER(f64), C.POINTER(f64), C.POINTER(f64)]),
+    "tff_server_release": (i32, [vp, i64]),
+    "tff_server_drain": (i32, [vp, f64]),
+    "tff_server_get_stats": (i32, [vp, C.POINTER(ServerStats)]),
 }
 
 for _name, (_res, _args) in _SIGS.items():
