@@ -245,23 +245,31 @@ def run_serving(device, n_requests: int = 4096, seed: int = 0) -> dict:
     srv = Server(rc, alpha, torch.float32, lanes=lanes, max_systems_per_batch=per_batch, hbm_budget_bytes=budget,
                  atoms_per_cell=apc, device=device)
 
+    prepared = [srv.prepare(sp) for sp in specs]
+
     def run(rate):
-        """Submit every request (all at once for rate None, else Poisson arrivals); latencies."""
-        t0 = time.perf_counter()
-        arrivals = None if rate is None else np.cumsum(np.random.default_rng(seed + 7).exponential(1.0 / rate,
-                                                                                                n_requests))
-        s0 = srv.now()
+        """rate None: every request queued while the server holds, then released at once
+        (throughput from release to the last completion; latency from release). Otherwise
+        Poisson arrivals at `rate` per second (latency from submission)."""
         reqs = []
-        for k, sp in enumerate(specs):
-            if arrivals is not None:
+        if rate is None:
+            srv.hold(True)
+            reqs = [srv.submit(pr) for pr in prepared]
+            s0 = srv.now()
+            srv.hold(False)
+        else:
+            arrivals = np.cumsum(np.random.default_rng(seed + 7).exponential(1.0 / rate, n_requests))
+            s0 = srv.now()
+            t0 = time.perf_counter()
+            for k, pr in enumerate(prepared):
                 while time.perf_counter() - t0 < arrivals[k]:
                     pass
-            reqs.append(srv.submit(sp))
+                reqs.append(srv.submit(pr))
         srv.drain()
         times = np.array([r.times() for r in reqs])
         for r in reqs:
             r.release()
-        lat = (times[:, 2] - times[:, 0]) * 1e3
+        lat = (times[:, 2] - np.maximum(times[:, 0], s0)) * 1e3
         span = times[:, 2].max() - s0
         return reqs, {"systems_per_s": round(n_requests / span, 1), "p50_ms": round(float(np.median(lat)), 3),
                       "p99_ms": round(float(np.percentile(lat, 99)), 3), "makespan_s": round(float(span), 4)}

@@ -243,6 +243,21 @@ int tff_timer_destroy(tff_timer timer);
 int tff_timer_elapsed_ms(tff_timer timer, int from, int to, float *ms);
 int tff_system_eval_timed(tff_system sys, const void *coords, const void *box, double *energy,
                           void *forces, tff_timer timer, tff_stream_t stream);
+/* First derivatives with respect to the per-atom parameters too (energy, forces = -dE/dx,
+ * dE/dq, dE/dsigma, dE/depsilon; any output may be NULL). Epsilon enters the LB mean as
+ * sqrt(eps_i eps_j); dE/deps_i is reported as 0 where eps_i = 0 (the derivative of sqrt is
+ * unbounded there). The reference's pair op divides by eps_ij instead
+ * (csrc/nonbonded/nonbonded_atom_pairs_cuda.cu:126-129). */
+int tff_system_eval_grads(tff_system sys, const void *coords, const void *box, double *energy, void *forces,
+                          void *grad_charges, void *grad_sigma, void *grad_epsilon, tff_stream_t stream);
+/* Second derivatives for force matching (no reference counterpart: the reference has no
+ * double backward on CUDA). For a coordinate direction u (N, 3) writes the derivatives of
+ * s(x, q, sigma, eps) = sum_i u_i . dE/dx_i with respect to the coordinates (N, 3), charges,
+ * sigma and epsilon (N each; NULL skips). One call rebuilds the cluster lists and evaluates
+ * the real-space and PME second derivatives (the PME part spreads the directional grid
+ * P = sum_i q_i u_i . grad theta_i and convolves it like the charge grid). */
+int tff_system_hvp(tff_system sys, const void *coords, const void *box, const void *direction, void *hvp_coords,
+                   void *hvp_charges, void *hvp_sigma, void *hvp_epsilon, tff_stream_t stream);
 /* Number of kernels of this library one tff_system_eval launches (cuFFT's excluded). */
 int tff_system_kernel_launches(tff_system sys);
 
@@ -350,6 +365,8 @@ int tff_server_release(tff_server server, int64_t ticket);
 /* Blocks until every submitted request is done. */
 int tff_server_drain(tff_server server, double timeout_s);
 int tff_server_get_stats(tff_server server, tff_server_stats *stats);
+/* hold != 0: no new batch starts (submissions keep queueing); hold == 0 resumes. */
+int tff_server_hold(tff_server server, int hold);
 
 #ifdef __cplusplus
 }

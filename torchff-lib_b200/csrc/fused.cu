@@ -28,8 +28,11 @@ struct tff_system_s {
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   void *cl_ws = nullptr;
   void *pme_ws = nullptr;
-  void *acc = nullptr;         // gx (npad*3), gq (npad): zeroed per evaluation
+  void *acc = nullptr;         // gx (npad*3), gq, gsigma, ga (npad each): zeroed per evaluation
   size_t acc_bytes = 0;
+  void *pme_ws2 = nullptr;     // second PME workspace (direction grid of second derivatives)
+  void *dir_sorted = nullptr;  // direction of a second-derivative pass per sorted slot
+  void *pme_hx = nullptr, *pme_hq = nullptr;  // PME second derivatives (caller order)
   void *lj = nullptr;          // sorted (sigma/2, sqrt eps)
   int *exslot = nullptr;       // sorted excluded-partner slots (npad, kMaxExcl)
   void *pme_grad = nullptr;    // PME dE/dx (N,3), caller order, e^2/nm units
@@ -108,7 +111,7 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
   if ((st = mark(1, s)) != TFF_OK) return st;
   S *gx = static_cast<S *>(sys->acc);
   S *gq = gx + 3 * sys->cl.npad;
-  TFF_CUDA(cudaMemsetAsync(sys->acc, 0, sys->acc_bytes, s));
+  TFF_CUDA(cudaMemsetAsync(sys->acc, 0, (size_t)sys->cl.npad * 4 * 8, s));
   auto *lj = static_cast<typename V2<T>::type *>(sys->lj);
   if (n > 0) {
     const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((sys->cl.npad + 255) / 256, sms * 8));
@@ -143,6 +146,131 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
   return mark(5, s);
 }
 
+// Sorted accumulators -> caller order for MODE 1 (out_x = forces, out_q/out_s/out_e =
+// dE/dq, dE/dsigma, dE/deps, energy) and MODE 2 (the same slots hold the derivatives of
+// dir . dE/dx). pme_vec / pme_scal are the PME parts (already scaled by kc in MODE 2).
+// dE/deps_i = (dE/da_i) / (2 a_i) with a = sqrt(eps), and 0 where eps_i = 0.
+template <class T, int MODE>
+__global__ void finalize_grads_kernel(ClusterData<T> cl, const typename Acc<T>::S *acc, const T *pme_vec,
+                                      const T *pme_scal, const T *eps, double kc, T *out_x, T *out_q, T *out_s,
+                                      T *out_e, const typename Acc<T>::S *e_tile, const double *e_pme,
+                                      double *energy) {
+  using S = typename Acc<T>::S;
+  const int64_t np = cl.npad;
+  const S *gx = acc, *gq = acc + 3 * np, *gs = acc + 4 * np, *ga = acc + 5 * np;
+  const double ps = MODE == 1 ? kc : 1.0;
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < cl.natoms; a += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = cl.inv[a];
+    double x[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x[c] = Acc<T>::get(&gx[3 * s + c]) + (pme_vec ? ps * (double)pme_vec[3 * a + c] : 0.0);
+    if (out_x)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) out_x[3 * a + c] = (T)(MODE == 1 ? -x[c] : x[c]);
+    if (out_q) out_q[a] = (T)(Acc<T>::get(&gq[s]) + (pme_scal ? ps * (double)pme_scal[a] : 0.0));
+    if (out_s) out_s[a] = (T)Acc<T>::get(&gs[s]);
+    if (out_e) {
+      const double ai = sqrt((double)eps[a]);
+      out_e[a] = (T)(ai > 0.0 ? Acc<T>::get(&ga[s]) / (2.0 * ai) : 0.0);
+    }
+  }
+  if (MODE == 1 && energy && blockIdx.x == 0 && threadIdx.x == 0) {
+    const double rec = e_pme ? kc * e_pme[0] : 0.0, self = e_pme ? kc * e_pme[1] : 0.0;
+    energy[0] = Acc<T>::get(&e_tile[0]) + Acc<T>::get(&e_tile[1]) + rec + self;
+  }
+}
+
+// MODE 1: energy, forces and parameter gradients. MODE 2: derivatives of dir . dE/dx with
+// respect to coordinates, charges, sigma and epsilon (one Hessian-vector product; the
+// cluster lists and both PME potentials are rebuilt for these coordinates).
+template <class T, int MODE>
+int system_grad_impl(tff_system sys, const T *x, const T *box, const T *dir, double *energy, T *out_x, T *out_q,
+                     T *out_s, T *out_e, cudaStream_t s) {
+  using S = typename Acc<T>::S;
+  const int64_t n = sys->desc.natoms;
+  const int sms = sm_count();
+  S *energies = reinterpret_cast<S *>(sys->scratch);
+  TFF_CUDA(cudaMemsetAsync(sys->scratch, 0, 8 * sizeof(double), s));
+  const bool use_pme = sys->pme && n > 0;
+  const double *e_pme = nullptr;
+  if (use_pme) {
+    TFF_CUDA(cudaEventRecord(sys->fork_ev, s));
+    TFF_CUDA(cudaStreamWaitEvent(sys->pme_stream, sys->fork_ev, 0));
+    cudaStream_t ps = sys->pme_stream;
+    const int K = sys->desc.pme_grid;
+    const T *xm = static_cast<const T *>(sys->moduli), *ym = xm + K, *zm = ym + K;
+    char *pw = static_cast<char *>(sys->pme_ws);
+    PlainAtoms<T> atoms{x, static_cast<const T *>(sys->q), n};
+    T *phi_grid = nullptr;
+    int st = pme_grid_phase<T>(sys->pme->impl, sys->pl, pw, atoms, n, box, sys->desc.ewald_alpha, xm, ym, zm, ps,
+                               &phi_grid);
+    if (st != TFF_OK) return st;
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((n * kLanesPerAtom + kPmeBlock - 1) / kPmeBlock, sms * 8));
+    if constexpr (MODE == 1) {
+      PlainGatherOut<T> out{static_cast<T *>(sys->pme_phi), static_cast<T *>(sys->pme_grad)};
+      st = pme_gather_phase<T>(sys->pme->impl, sys->pl, pw, atoms, n, box, sys->desc.ewald_alpha, phi_grid, out, 1.0,
+                               (T *)nullptr, ps);
+      if (st != TFF_OK) return st;
+      e_pme = reinterpret_cast<const double *>(pw + sys->pl.energies);
+    } else {
+      char *pw2 = static_cast<char *>(sys->pme_ws2);
+      TFF_CUDA(cudaMemsetAsync(pw2 + sys->pl.zero_off, 0, sys->pl.zero_bytes, ps));
+      pme_spread_dir_kernel<T><<<nb, kPmeBlock, 0, ps>>>(atoms, dir, n, box, K,
+                                                         reinterpret_cast<S *>(pw2 + sys->pl.fix));
+      TFF_LAUNCHED();
+      T *psi_grid = nullptr;
+      st = pme_solve_phase<T>(sys->pme->impl, sys->pl, pw2, box, sys->desc.ewald_alpha, xm, ym, zm, ps, &psi_grid);
+      if (st != TFF_OK) return st;
+      pme_gather_hvp_kernel<T><<<nb, kPmeBlock, 0, ps>>>(atoms, dir, n, box, K, phi_grid, psi_grid,
+                                                         sys->desc.coul_constant, static_cast<T *>(sys->pme_hx),
+                                                         static_cast<T *>(sys->pme_hq));
+      TFF_LAUNCHED();
+    }
+    TFF_CUDA(cudaEventRecord(sys->join_ev, ps));
+  }
+  ClusterData<T> cd = cluster_data<T>(sys->cl, sys->cl_ws);
+  int st = build_clusters<T>(sys->cl, cd, sys->cl_ws, x, static_cast<const T *>(sys->q), box, sys->desc.cutoff, 0, s);
+  if (st != TFF_OK) return st;
+  S *acc = static_cast<S *>(sys->acc);
+  const int64_t np = sys->cl.npad;
+  TFF_CUDA(cudaMemsetAsync(sys->acc, 0, (size_t)np * 6 * 8, s));
+  auto *lj = static_cast<typename V2<T>::type *>(sys->lj);
+  auto *dsorted = static_cast<typename V4<T>::type *>(sys->dir_sorted);
+  if (n > 0) {
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((np + 255) / 256, sms * 8));
+    sorted_params_kernel<T><<<nb, 256, 0, s>>>(cd, static_cast<const T *>(sys->sigma), static_cast<const T *>(sys->eps),
+                                               sys->excl, lj, sys->exslot, MODE == 2 ? dir : nullptr, dsorted);
+    TFF_LAUNCHED();
+    TileArgs<T> A;
+    A.cl = cd;
+    A.lj = lj;
+    A.exslot = sys->exslot;
+    A.gx = acc;
+    A.gq = acc + 3 * np;
+    A.gs = acc + 4 * np;
+    A.ga = acc + 5 * np;
+    A.u = dsorted;
+    A.rc = sys->desc.cutoff;
+    A.alpha = sys->desc.ewald_alpha;
+    A.kc = sys->desc.coul_constant;
+    A.energies = energies;
+    const int64_t max_items = sys->cl.nclusters * ((sys->cl.cap + kItemTiles - 1) / kItemTiles);
+    constexpr int NW = TileCfg<T, MODE>::NW;
+    const int nbt = (int)std::max<int64_t>(1, std::min<int64_t>((max_items + NW - 1) / NW, (int64_t)sms * 48 / NW));
+    tile_kernel<T, MODE><<<nbt, NW * kWarp, 0, s>>>(A);
+    TFF_LAUNCHED();
+  }
+  if (use_pme) TFF_CUDA(cudaStreamWaitEvent(s, sys->join_ev, 0));
+  const T *pvec = use_pme ? static_cast<const T *>(MODE == 1 ? sys->pme_grad : sys->pme_hx) : nullptr;
+  const T *pscal = use_pme ? static_cast<const T *>(MODE == 1 ? sys->pme_phi : sys->pme_hq) : nullptr;
+  const int nbf = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sms * 8));
+  finalize_grads_kernel<T, MODE><<<nbf, 256, 0, s>>>(cd, acc, pvec, pscal, static_cast<const T *>(sys->eps),
+                                                     sys->desc.coul_constant, out_x, out_q, out_s, out_e, energies,
+                                                     e_pme, energy);
+  TFF_LAUNCHED();
+  return TFF_OK;
+}
+
 template <class T>
 int set_params_impl(tff_system sys, const T *q, const T *sig, const T *eps, cudaStream_t s) {
   const size_t bytes = sizeof(T) * sys->desc.natoms;
@@ -160,7 +288,8 @@ void free_system(tff_system sys) {
   if (sys->join_ev) cudaEventDestroy(sys->join_ev);
   if (sys->host_graph) cudaGraphExecDestroy(sys->host_graph);
   if (sys->capture_stream) cudaStreamDestroy(sys->capture_stream);
-  void *ptrs[] = {sys->cl_ws, sys->pme_ws, sys->acc, sys->lj, sys->exslot, sys->pme_grad, sys->pme_phi,
+  void *ptrs[] = {sys->cl_ws, sys->pme_ws, sys->pme_ws2, sys->dir_sorted, sys->pme_hx, sys->pme_hq,
+                  sys->acc, sys->lj, sys->exslot, sys->pme_grad, sys->pme_phi,
                   sys->q, sys->sigma, sys->eps, sys->excl, sys->moduli, sys->scratch, sys->host_x,
                   sys->dev_x, sys->dev_f, sys->dev_e};
   for (void *p : ptrs)
@@ -218,8 +347,11 @@ int tff_system_create(const tff_system_desc *desc, const double *charges, const 
     }                                                                      \
   } while (0)
   TFF_ALLOC(sys->cl_ws, sys->cl.bytes);
-  sys->acc_bytes = (size_t)sys->cl.npad * 4 * 8;
+  sys->acc_bytes = (size_t)sys->cl.npad * 6 * 8;
   TFF_ALLOC(sys->acc, sys->acc_bytes);
+  TFF_ALLOC(sys->dir_sorted, (size_t)sys->cl.npad * 4 * ts);
+  TFF_ALLOC(sys->pme_hx, 3 * n * ts);
+  TFF_ALLOC(sys->pme_hq, n * ts);
   TFF_ALLOC(sys->lj, (size_t)sys->cl.npad * 2 * ts);
   TFF_ALLOC(sys->exslot, (size_t)sys->cl.npad * kMaxExcl * sizeof(int));
   TFF_ALLOC(sys->pme_grad, 3 * n * ts);
@@ -264,6 +396,7 @@ int tff_system_create(const tff_system_desc *desc, const double *charges, const 
     }
     sys->pl = pme_layout(desc->dtype, K);
     TFF_ALLOC(sys->pme_ws, sys->pl.bytes);
+    TFF_ALLOC(sys->pme_ws2, sys->pl.bytes);
     TFF_ALLOC(sys->moduli, (size_t)(2 * K + K / 2 + 1) * ts);
     std::vector<double> mod;
     auto mx = host_moduli(K, K);
@@ -273,6 +406,7 @@ int tff_system_create(const tff_system_desc *desc, const double *charges, const 
     mod.insert(mod.end(), mz.begin(), mz.end());
     upload(sys->moduli, mod.data(), (int64_t)mod.size());
     if (e == cudaSuccess) e = cudaMemset(sys->pme_ws, 0, sys->pl.bytes);
+    if (e == cudaSuccess) e = cudaMemset(sys->pme_ws2, 0, sys->pl.bytes);
     if (e != cudaSuccess) {
       free_system(sys);
       return cuda_fail(e, "upload moduli", __FILE__, __LINE__);
@@ -401,6 +535,33 @@ int tff_system_eval_timed(tff_system sys, const void *coords, const void *box, d
                                    nullptr, nullptr, s, timer->ev);
   return system_eval_impl<double>(sys, (const double *)coords, (const double *)box, energy, (double *)forces,
                                   nullptr, nullptr, nullptr, s, timer->ev);
+}
+
+int tff_system_eval_grads(tff_system sys, const void *coords, const void *box, double *energy, void *forces,
+                          void *grad_charges, void *grad_sigma, void *grad_epsilon, tff_stream_t stream) {
+  TFF_ARG(sys != nullptr && box != nullptr, "system/box is NULL");
+  TFF_ARG(sys->desc.natoms == 0 || coords != nullptr, "coords is NULL");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (sys->desc.dtype == TFF_F32)
+    return system_grad_impl<float, 1>(sys, (const float *)coords, (const float *)box, nullptr, energy, (float *)forces,
+                                      (float *)grad_charges, (float *)grad_sigma, (float *)grad_epsilon, s);
+  return system_grad_impl<double, 1>(sys, (const double *)coords, (const double *)box, nullptr, energy,
+                                     (double *)forces, (double *)grad_charges, (double *)grad_sigma,
+                                     (double *)grad_epsilon, s);
+}
+
+int tff_system_hvp(tff_system sys, const void *coords, const void *box, const void *direction, void *hvp_coords,
+                   void *hvp_charges, void *hvp_sigma, void *hvp_epsilon, tff_stream_t stream) {
+  TFF_ARG(sys != nullptr && box != nullptr, "system/box is NULL");
+  TFF_ARG(sys->desc.natoms == 0 || (coords != nullptr && direction != nullptr), "coords/direction is NULL");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (sys->desc.dtype == TFF_F32)
+    return system_grad_impl<float, 2>(sys, (const float *)coords, (const float *)box, (const float *)direction,
+                                      nullptr, (float *)hvp_coords, (float *)hvp_charges, (float *)hvp_sigma,
+                                      (float *)hvp_epsilon, s);
+  return system_grad_impl<double, 2>(sys, (const double *)coords, (const double *)box, (const double *)direction,
+                                     nullptr, (double *)hvp_coords, (double *)hvp_charges, (double *)hvp_sigma,
+                                     (double *)hvp_epsilon, s);
 }
 
 int tff_system_kernel_launches(tff_system sys) {

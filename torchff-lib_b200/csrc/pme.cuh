@@ -290,6 +290,144 @@ __global__ void __launch_bounds__(kPmeBlock) pme_gather_kernel(Atoms atoms, int6
   if (last && threadIdx.x == 0 && energy_out) energy_out[0] = (T)(e_scale * (*e_rec + *e_self));
 }
 
+// ---- second derivatives along a coordinate direction u (force matching)
+// With theta_i(g) the stencil weight and w_d = m0_d - u_d its spline argument
+// (dw_d/dr_c = -recip[d][c]), v_i = recip u_i, G_d = d theta / d w_d, H_de = d2 theta / dw_d dw_e:
+//   P(g)   = sum_i q_i u_i . grad theta_i(g) = -sum_i q_i sum_d v_d G_d(g)
+//   psi    = the same influence-function convolution of P as Phi of Q
+//   d/dx_i (sum_j u_j . dE/dx_j) = q_i recip^T (A v_i - B),  A_de = sum_g Phi H_de, B_d = sum_g psi G_d
+//   d/dq_i (sum_j u_j . dE/dx_j) = -v_i . C + sum_g psi theta_i,  C_d = sum_g Phi G_d
+// (the reciprocal energy is 1/2 Q.Phi; the self term has no coordinate dependence).
+template <class T>
+__global__ void __launch_bounds__(kPmeBlock) pme_spread_dir_kernel(PlainAtoms<T> atoms, const T *dir, int64_t n,
+                                                                   const T *box, int K, typename Acc<T>::S *grid) {
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
+  __syncthreads();
+  const int g = threadIdx.x % kLanesPerAtom;
+  const int64_t wglob = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  const int64_t nwarps = (int64_t)gridDim.x * blockDim.x / kWarp;
+  for (int64_t wb = wglob * kAtomsPerWarp; wb < n; wb += nwarps * kAtomsPerWarp) {
+    const int64_t t = wb + (threadIdx.x % kWarp) / kLanesPerAtom;
+    double rx, ry, rz;
+    T q;
+    if (t >= n || !atoms.get(t, rx, ry, rz, q)) continue;
+    const double ux = dir[3 * t], uy = dir[3 * t + 1], uz = dir[3 * t + 2];
+    const double v0 = sh.recip[0] * ux + sh.recip[1] * uy + sh.recip[2] * uz;
+    const double v1 = sh.recip[3] * ux + sh.recip[4] * uy + sh.recip[5] * uz;
+    const double v2 = sh.recip[6] * ux + sh.recip[7] * uy + sh.recip[8] * uz;
+    Stencil<T> s;
+    make_stencil<T>(rx, ry, rz, sh.recip, K, s);
+    for (int r = g; r < 36; r += kLanesPerAtom) {
+      const int a = r / 6, b = r % 6;
+      int gx = s.g0[0] + a, gy = s.g0[1] + b;
+      gx -= (gx >= K) ? K : 0;
+      gy -= (gy >= K) ? K : 0;
+      const double wx = s.val[0][a], dx = s.der[0][a], wy = s.val[1][b], dy = s.der[1][b];
+      const double c_val = -(double)q * (v0 * dx * wy + v1 * wx * dy);  // times val_z
+      const double c_der = -(double)q * v2 * wx * wy;                    // times der_z
+      const int64_t row = ((int64_t)gx * K + gy) * K;
+      int gz = s.g0[2];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        Acc<T>::add(&grid[row + gz], c_val * (double)s.val[2][c] + c_der * (double)s.der[2][c]);
+        gz = (gz + 1 == K) ? 0 : gz + 1;
+      }
+    }
+  }
+}
+
+// Per atom: kc * d/dx_i and kc * d/dq_i of sum_j u_j . dE_rec/dx_j (kLanesPerAtom lanes per atom).
+template <class T>
+__global__ void __launch_bounds__(kPmeBlock) pme_gather_hvp_kernel(PlainAtoms<T> atoms, const T *dir, int64_t n,
+                                                                   const T *box, int K, const T *Phi, const T *Psi,
+                                                                   double kc, T *hx, T *hq) {
+  __shared__ PmeShared sh;
+  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
+  __syncthreads();
+  const int g = threadIdx.x % kLanesPerAtom;
+  const int64_t wglob = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  const int64_t nwarps = (int64_t)gridDim.x * blockDim.x / kWarp;
+  for (int64_t wb = wglob * kAtomsPerWarp; wb < n; wb += nwarps * kAtomsPerWarp) {
+    const int64_t t = wb + (threadIdx.x % kWarp) / kLanesPerAtom;
+    double rx = 0.0, ry = 0.0, rz = 0.0;
+    T q = T(0);
+    const bool ok = t < n && atoms.get(t, rx, ry, rz, q);
+    // A00 A11 A22 A01 A02 A12, B0..2, C0..2, Psi_i
+    double acc[13];
+#pragma unroll
+    for (int k = 0; k < 13; ++k) acc[k] = 0.0;
+    T val[3][6], der[3][6], dd[3][6];
+    int g0[3];
+    if (ok) {
+      const double r[3] = {rx, ry, rz};
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double u = sh.recip[3 * d] * r[0] + sh.recip[3 * d + 1] * r[1] + sh.recip[3 * d + 2] * r[2];
+        const double m0 = ceil(u);
+        bspline6_d2<T>((T)(m0 - u), val[d], der[d], dd[d]);
+        long long gg = (long long)m0 - 3;
+        gg %= K;
+        if (gg < 0) gg += K;
+        g0[d] = (int)gg;
+      }
+      for (int rr = g; rr < 36; rr += kLanesPerAtom) {
+        const int a = rr / 6, b = rr % 6;
+        int gx = g0[0] + a, gy = g0[1] + b;
+        gx -= (gx >= K) ? K : 0;
+        gy -= (gy >= K) ? K : 0;
+        const int64_t row = ((int64_t)gx * K + gy) * K;
+        int gz = g0[2];
+        double pv = 0.0, pd = 0.0, pdd = 0.0, sv = 0.0, sd = 0.0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          const double ph = Phi[row + gz], ps = Psi[row + gz];
+          pv += ph * (double)val[2][c];
+          pd += ph * (double)der[2][c];
+          pdd += ph * (double)dd[2][c];
+          sv += ps * (double)val[2][c];
+          sd += ps * (double)der[2][c];
+          gz = (gz + 1 == K) ? 0 : gz + 1;
+        }
+        const double vx = val[0][a], dx = der[0][a], ddx = dd[0][a];
+        const double vy = val[1][b], dy = der[1][b], ddy = dd[1][b];
+        acc[0] += ddx * vy * pv;
+        acc[1] += vx * ddy * pv;
+        acc[2] += vx * vy * pdd;
+        acc[3] += dx * dy * pv;
+        acc[4] += dx * vy * pd;
+        acc[5] += vx * dy * pd;
+        acc[6] += dx * vy * sv;
+        acc[7] += vx * dy * sv;
+        acc[8] += vx * vy * sd;
+        acc[9] += dx * vy * pv;
+        acc[10] += vx * dy * pv;
+        acc[11] += vx * vy * pd;
+        acc[12] += vx * vy * sv;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 13; ++k)
+#pragma unroll
+      for (int o = kLanesPerAtom / 2; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(kFull, acc[k], o);
+    if (ok && g == 0) {
+      const double ux = dir[3 * t], uy = dir[3 * t + 1], uz = dir[3 * t + 2];
+      double v[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) v[d] = sh.recip[3 * d] * ux + sh.recip[3 * d + 1] * uy + sh.recip[3 * d + 2] * uz;
+      const double A[3][3] = {{acc[0], acc[3], acc[4]}, {acc[3], acc[1], acc[5]}, {acc[4], acc[5], acc[2]}};
+      double w[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) w[d] = A[d][0] * v[0] + A[d][1] * v[1] + A[d][2] * v[2] - acc[6 + d];
+      const double qd = (double)q;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        hx[3 * t + c] = (T)(kc * qd * (sh.recip[c] * w[0] + sh.recip[3 + c] * w[1] + sh.recip[6 + c] * w[2]));
+      hq[t] = (T)(kc * (-(v[0] * acc[9] + v[1] * acc[10] + v[2] * acc[11]) + acc[12]));
+    }
+  }
+}
+
 // ---- batched PME: blockIdx.y is the system, blocks [0, BatchSys::pme_blocks) of it work
 // (a count that depends on the system alone, so that its reductions sum in the same order
 // whatever else is in the batch).
@@ -389,22 +527,15 @@ struct tff_pme_plan_s {
 
 namespace tff {
 
-// Enqueue spread -> FFT -> convolve -> FFT on `s`; leaves the potential grid Phi in
-// (T*)(ws + L.real) (mixed) or (T*)(ws + L.fix) (FP64) and returns it through *phi_grid.
-template <class T, class Atoms>
-int pme_grid_phase(const PmePlanImpl &p, const PmeLayout &L, char *ws, Atoms atoms, int64_t nthreads, const T *box,
-                   double alpha, const T *xmod, const T *ymod, const T *zmod, cudaStream_t s, T **phi_grid) {
+// FFT -> convolve -> FFT of the spread grid in ws (L.fix) on `s`; leaves the potential grid
+// Phi in (T*)(ws + L.real) (mixed) or (T*)(ws + L.fix) (FP64), returned through *phi_grid.
+template <class T>
+int pme_solve_phase(const PmePlanImpl &p, const PmeLayout &L, char *ws, const T *box, double alpha, const T *xmod,
+                    const T *ymod, const T *zmod, cudaStream_t s, T **phi_grid) {
   using S = typename Acc<T>::S;
   const int K = p.K;
-  TFF_CUDA(cudaMemsetAsync(ws + L.zero_off, 0, L.zero_bytes, s));
   const int sms = sm_count();
   S *grid = reinterpret_cast<S *>(ws + L.fix);
-  if (nthreads > 0) {
-    const int64_t lanes = nthreads * kLanesPerAtom;
-    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((lanes + kPmeBlock - 1) / kPmeBlock, sms * 8));
-    pme_spread_kernel<T, Atoms><<<nb, kPmeBlock, 0, s>>>(atoms, nthreads, box, K, grid);
-    TFF_LAUNCHED();
-  }
   T *real;
   if (sizeof(T) == 4) {
     real = reinterpret_cast<T *>(ws + L.real);
@@ -440,6 +571,22 @@ int pme_grid_phase(const PmePlanImpl &p, const PmeLayout &L, char *ws, Atoms ato
   if (r != CUFFT_SUCCESS) return pme_cufft_fail(r, "inverse FFT");
   *phi_grid = real;
   return TFF_OK;
+}
+
+// Enqueue spread -> FFT -> convolve -> FFT on `s` (see pme_solve_phase for the result).
+template <class T, class Atoms>
+int pme_grid_phase(const PmePlanImpl &p, const PmeLayout &L, char *ws, Atoms atoms, int64_t nthreads, const T *box,
+                   double alpha, const T *xmod, const T *ymod, const T *zmod, cudaStream_t s, T **phi_grid) {
+  using S = typename Acc<T>::S;
+  TFF_CUDA(cudaMemsetAsync(ws + L.zero_off, 0, L.zero_bytes, s));
+  S *grid = reinterpret_cast<S *>(ws + L.fix);
+  if (nthreads > 0) {
+    const int64_t lanes = nthreads * kLanesPerAtom;
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((lanes + kPmeBlock - 1) / kPmeBlock, sm_count() * 8));
+    pme_spread_kernel<T, Atoms><<<nb, kPmeBlock, 0, s>>>(atoms, nthreads, box, p.K, grid);
+    TFF_LAUNCHED();
+  }
+  return pme_solve_phase<T>(p, L, ws, box, alpha, xmod, ymod, zmod, s, phi_grid);
 }
 
 template <class T, class Atoms, class Out>

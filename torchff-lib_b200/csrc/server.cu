@@ -73,6 +73,7 @@ struct tff_server_s {
   std::condition_variable cv_work, cv_done;
   std::thread worker;
   bool stop = false;
+  bool hold = false;  // no new batch starts while set (requests keep queueing)
   int fatal = TFF_OK;
   std::chrono::steady_clock::time_point t0;
   tff_server_stats stats{};
@@ -224,7 +225,7 @@ void worker_loop(tff_server s) {
       s->cv_done.notify_all();
     }
     for (Lane &l : s->lanes) {
-      if (l.busy || s->queue.empty() || s->fatal != TFF_OK) continue;
+      if (l.busy || s->queue.empty() || s->fatal != TFF_OK || s->hold) continue;
       int64_t atoms = 0, grid = 0;
       while (!s->queue.empty() && (int)l.reqs.size() < l.max_systems) {
         ServerReq *r = s->queue.front();
@@ -279,7 +280,7 @@ void worker_loop(tff_server s) {
     if (s->stop && !any_busy && (s->queue.empty() || s->fatal != TFF_OK)) break;
     if (progress) continue;
     if (!any_busy) {
-      s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+      s->cv_work.wait(lk, [&] { return s->stop || (!s->queue.empty() && !s->hold); });
     } else {
       lk.unlock();
       std::this_thread::yield();
@@ -294,6 +295,7 @@ void free_server(tff_server s) {
     {
       std::lock_guard<std::mutex> g(s->mu);
       s->stop = true;
+      s->hold = false;
     }
     s->cv_work.notify_all();
     s->worker.join();
@@ -506,6 +508,16 @@ int tff_server_drain(tff_server s, double timeout_s) {
     return TFF_ERR_TIMEOUT;
   }
   return s->fatal;
+}
+
+int tff_server_hold(tff_server s, int hold) {
+  TFF_ARG(s != nullptr, "server is NULL");
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->hold = hold != 0;
+  }
+  s->cv_work.notify_all();
+  return TFF_OK;
 }
 
 int tff_server_get_stats(tff_server s, tff_server_stats *out) {

@@ -247,4 +247,43 @@ __device__ __forceinline__ void bspline6(T w, T val[6], T der[6]) {
   }
 }
 
+// As bspline6, plus the second derivative dd[k] = M6''(w + k), from
+// M_n''(u) = M_{n-2}(u) - 2 M_{n-2}(u - 1) + M_{n-2}(u - 2) with M4 taken inside the recursion.
+template <class T>
+__device__ __forceinline__ void bspline6_d2(T w, T val[6], T der[6], T dd[6]) {
+  T m[6], m4[6];
+  m[0] = w;
+  m[1] = T(1) - w;
+#pragma unroll
+  for (int n = 3; n <= 5; ++n) {
+    T inv = T(1) / T(n - 1);
+    T prev = T(0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      if (k < n) {
+        T u = w + T(k);
+        T cur = (k < n - 1) ? m[k] : T(0);
+        T nv = (u * cur + (T(n) - u) * prev) * inv;
+        prev = cur;
+        m[k] = nv;
+      }
+    }
+    if (n == 4) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) m4[k] = k < 4 ? m[k] : T(0);  // M4(w + k)
+    }
+  }
+  T prev = T(0);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    T cur = (k < 5) ? m[k] : T(0);
+    der[k] = cur - prev;
+    T u = w + T(k);
+    val[k] = (u * cur + (T(6) - u) * prev) * (T(1) / T(5));
+    prev = cur;
+    const T a = m4[k], b = k >= 1 ? m4[k - 1] : T(0), c = k >= 2 ? m4[k - 2] : T(0);
+    dd[k] = a - T(2) * b + c;
+  }
+}
+
 }  // namespace tff

@@ -29,7 +29,11 @@ constexpr int kMaxExcl = 8;       // excluded partners per atom (self excluded)
 
 // Warps per block of the tile kernel: 4 (FP32) or 2 (FP64) so that the staged tiles fit in
 // 48 KB of static shared memory.
-template <class T> struct TileCfg { static constexpr int NW = sizeof(T) == 8 ? 2 : 4; };
+// MODE 0: energy, dE/dx, dE/dq. MODE 1: also dE/dsigma and dE/d(sqrt eps). MODE 2: second
+// derivatives along a coordinate direction u: d/dx, d/dq, d/dsigma, d/d(sqrt eps) of u . dE/dx.
+template <class T, int MODE = 0> struct TileCfg {
+  static constexpr int NW = (sizeof(T) == 8 || MODE == 2) ? 2 : 4;
+};
 
 template <class T> struct V2;
 template <> struct V2<float> { using type = float2; };
@@ -41,11 +45,13 @@ __device__ __forceinline__ D2 make_v2(double a, double b) { return D2{a, b}; }
 __device__ __forceinline__ float erf_t(float x) { return erff(x); }
 __device__ __forceinline__ double erf_t(double x) { return erf(x); }
 
-// erfc(u) and exp(-u^2) of the FP64 path (the FP32 path inlines A&S 7.1.26 in pass 2).
+// erfc(u) and exp(-u^2): libdevice in FP64, A&S 7.1.26 in FP32 (the MODE 0 FP32 path inlines
+// the same approximation with paired instructions).
 __device__ __forceinline__ void erfc_exp(double u, double &ec, double &ex) {
   ec = erfc(u);
   ex = exp(-u * u);
 }
+__device__ __forceinline__ void erfc_exp(float u, float &ec, float &ex) { erfc_exp_as(u, ec, ex); }
 __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 
@@ -58,15 +64,24 @@ struct TileArgs {
   typename Acc<T>::S *gq;          // (npad) sorted slots, dE/dq
   double rc, alpha, kc;
   typename Acc<T>::S *energies;    // per system: [2s] pairs (LJ + erfc Coulomb), [2s+1] exclusion correction
+  typename Acc<T>::S *gs = nullptr;  // MODE 1/2: (npad) d/dsigma_i
+  typename Acc<T>::S *ga = nullptr;  // MODE 1/2: (npad) d/da_i, a = sqrt(eps)
+  const typename V4<T>::type *u = nullptr;  // MODE 2: direction per sorted slot
 };
 
 // LB parameters and excluded-partner slots in sorted order. Partner indices are counted
 // from the first atom of the atom's own system (batch mode), i.e. global for one system.
+// With `dir` (caller order (N,3)) also the direction of a second-derivative pass in
+// sorted order.
 template <class T>
 __global__ void sorted_params_kernel(ClusterData<T> cl, const T *sigma, const T *eps, const int *excl,
-                                     typename V2<T>::type *lj, int *exslot) {
+                                     typename V2<T>::type *lj, int *exslot, const T *dir = nullptr,
+                                     typename V4<T>::type *dir_sorted = nullptr) {
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < cl.npad; s += (int64_t)gridDim.x * blockDim.x) {
     const int a = cl.sidx[s];
+    if (dir)
+      dir_sorted[s] = a >= 0 ? make_v4(dir[3 * (int64_t)a], dir[3 * (int64_t)a + 1], dir[3 * (int64_t)a + 2], T(0))
+                             : make_v4(T(0), T(0), T(0), T(0));
     const int64_t base = (cl.sys && a >= 0) ? cl.sys[cl.cl_sys[s / kWarp]].atom_off : 0;
     lj[s] = a >= 0 ? make_v2(T(0.5) * sigma[a], (T)sqrt((double)eps[a])) : make_v2(T(0), T(0));
 #pragma unroll
@@ -88,12 +103,13 @@ __device__ __forceinline__ void pair_min_image(bool ortho, T &dx, T &dy, T &dz, 
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(TileCfg<T>::NW * 32) tile_kernel(TileArgs<T> A) {
+template <class T, int MODE = 0>
+__global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32) tile_kernel(TileArgs<T> A) {
   using V = typename V4<T>::type;
   using W2 = typename V2<T>::type;
-  constexpr int NW = TileCfg<T>::NW;
+  constexpr int NW = TileCfg<T, MODE>::NW;
   __shared__ V s_pos[NW][kItemTiles][kWarp];
+  __shared__ V s_u[NW][kItemTiles][MODE == 2 ? kWarp : 1];  // MODE 2: direction of the j atoms
   __shared__ W2 s_lj[NW][kItemTiles][kWarp];
   // negated j positions, structure of arrays, for the packed FP32 distance pass
   __shared__ __align__(8) float s_nx[NW][kItemTiles][sizeof(T) == 4 ? kWarp : 2];
@@ -138,6 +154,8 @@ __global__ void __launch_bounds__(TileCfg<T>::NW * 32) tile_kernel(TileArgs<T> A
     const W2 lji = A.lj[si];
     const T kqi = kc * pi.w;
     const V ci = cl.bc[I], hi_ = cl.bh[I];
+    V ui{};
+    if constexpr (MODE == 2) ui = A.u[si];
 
     // stage the tiles and build their cutoff masks (pass 1)
     for (int t = 0; t < ntile; ++t) {
@@ -165,6 +183,7 @@ __global__ void __launch_bounds__(TileCfg<T>::NW * 32) tile_kernel(TileArgs<T> A
       }
       s_pos[w][t][lane] = pj;
       s_lj[w][t][lane] = A.lj[sj];
+      if constexpr (MODE == 2) s_u[w][t][lane] = A.u[sj];
       if (sizeof(T) == 4) {
         s_nx[w][t][lane] = -(float)pj.x;
         s_ny[w][t][lane] = -(float)pj.y;
@@ -220,7 +239,8 @@ __global__ void __launch_bounds__(TileCfg<T>::NW * 32) tile_kernel(TileArgs<T> A
     // pass 2: every lane walks its own in-cutoff pairs across all tiles of the item
     T fx = T(0), fy = T(0), fz = T(0), dq = T(0);
     double ep = 0.0;
-    if constexpr (sizeof(T) == 4) {
+    T d_sig = T(0), d_a = T(0);  // MODE 1/2: sigma and sqrt(eps) derivatives of atom i
+    if constexpr (MODE == 0 && sizeof(T) == 4) {
       // FP32: two pairs per iteration with paired instructions (FADD2/FMUL2/FFMA2); only
       // rsqrt, reciprocal and exp2 stay scalar. A lane with an odd count pads the second
       // slot with a zero-charge, zero-epsilon copy of the first, which contributes nothing.
@@ -305,6 +325,66 @@ __global__ void __launch_bounds__(TileCfg<T>::NW * 32) tile_kernel(TileArgs<T> A
       fy = fy2.x + fy2.y;
       fz = fz2.x + fz2.y;
       dq = dq2.x + dq2.y;
+    } else if constexpr (MODE != 0) {
+      // one pair per step. With D = (dE/dr)/r of the pair: MODE 1 adds dE/dsigma_i and
+      // dE/da_i; MODE 2 accumulates, with delta = u_i - u_j and rd = r_ij . delta,
+      // d/dx_i (u . dE/dx) = D delta + (dD/dr / r) rd r_ij and the parameter derivatives
+      // (dD/dp) rd (coordinates: fx..fz, charge: dq (times k later), sigma: d_sig, a: d_a)
+      T te = T(0);
+      int t = 0, iter = 0;
+      unsigned m = ntile > 0 ? s_mask[w][0][lane] : 0u;
+      while (true) {
+        while (m == 0u && ++t < ntile) m = s_mask[w][t][lane];
+        const bool have = m != 0u;
+        if (!__any_sync(kFull, have)) break;
+        if (MODE == 1 && (++iter & 15) == 0) {
+          ep += (double)te;
+          te = T(0);
+        }
+        if (have) {
+          const int s = __ffs(m) - 1;
+          m &= m - 1u;
+          const V q = s_pos[w][t][s];
+          const W2 ljj = s_lj[w][t][s];
+          T dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+          if (s_mi[w][t]) pair_min_image(ortho, dx, dy, dz, s_m, s_inv);
+          const T r2 = dx * dx + dy * dy + dz * dz;
+          const T rinv = rsqrt_t(r2);
+          const T rinv2 = rinv * rinv;
+          const T u = alpha * (r2 * rinv);
+          T ec, ex2;
+          erfc_exp(u, ec, ex2);
+          const T sig = lji.x + ljj.x, aj = ljj.y, eps = lji.y * aj;
+          const T sr = sig * rinv, sr2 = sr * sr, sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6, s5 = sr2 * sr2 * sr;
+          const T dcq = -q.w * (ec * rinv2 + two_a_rpi * ex2 * rinv) * rinv;  // D_coulomb / (k q_i)
+          const T dlj = T(-24) * eps * (T(2) * sr12 - sr6) * rinv2;           // D_lj
+          const T D = kqi * dcq + dlj;
+          if constexpr (MODE == 1) {
+            fx += D * dx;
+            fy += D * dy;
+            fz += D * dz;
+            dq += q.w * ec * rinv;
+            te += kqi * q.w * ec * rinv + T(4) * eps * (sr12 - sr6);
+            d_sig += T(12) * eps * rinv * s5 * (T(2) * sr6 - T(1));  // 1/2 dE/dsigma_ij
+            d_a += T(4) * aj * (sr12 - sr6);                       // dE/da_i
+          } else {
+            const V uj = s_u[w][t][s];
+            const T ddx = ui.x - uj.x, ddy = ui.y - uj.y, ddz = ui.z - uj.z;
+            const T rd = dx * ddx + dy * ddy + dz * ddz;
+            const T rinv4 = rinv2 * rinv2;
+            const T e2 = kqi * q.w * (T(3) * ec * rinv4 * rinv + two_a_rpi * ex2 * (T(3) * rinv4 + T(2) * alpha * alpha * rinv2)) +
+                         T(24) * eps * (T(28) * sr12 - T(8) * sr6) * rinv4;  // (dD/dr) / r
+            const T e2rd = e2 * rd;
+            fx += D * ddx + e2rd * dx;
+            fy += D * ddy + e2rd * dy;
+            fz += D * ddz + e2rd * dz;
+            dq += dcq * rd;
+            d_sig += T(-72) * eps * rinv2 * rinv * s5 * (T(4) * sr6 - T(1)) * rd;  // 1/2 dD/dsigma_ij rd
+            d_a += T(-24) * aj * (T(2) * sr12 - sr6) * rinv2 * rd;              // dD/da_i rd
+          }
+        }
+      }
+      ep += (double)te;
     } else {
       T te = T(0);  // partial energy, moved into ep every 16 pairs
       int t = 0, iter = 0;
@@ -367,12 +447,26 @@ __global__ void __launch_bounds__(TileCfg<T>::NW * 32) tile_kernel(TileArgs<T> A
         const T damp = -erf_t(u);
         const T ex2 = exp(-u * u);
         const T cq = q.w * damp * rinv;
-        const T dedr_r = -kqi * q.w * (damp * rinv * rinv + two_a_rpi * ex2 * rinv) * rinv;
-        fx += dedr_r * dx;
-        fy += dedr_r * dy;
-        fz += dedr_r * dz;
-        dq += cq;
-        ex += (double)(kqi * cq);
+        const T dcq = -q.w * (damp * rinv * rinv + two_a_rpi * ex2 * rinv) * rinv;
+        const T dedr_r = kqi * dcq;
+        if constexpr (MODE == 2) {
+          // same form as the erfc term with erfc(u) -> erfc(u) - 1 (equal derivatives)
+          const V uj = s_u[w][t][s];
+          const T ddx = ui.x - uj.x, ddy = ui.y - uj.y, ddz = ui.z - uj.z;
+          const T rd = dx * ddx + dy * ddy + dz * ddz;
+          const T rinv2 = rinv * rinv, rinv4 = rinv2 * rinv2;
+          const T e2rd = kqi * q.w * (T(3) * damp * rinv4 * rinv + two_a_rpi * ex2 * (T(3) * rinv4 + T(2) * alpha * alpha * rinv2)) * rd;
+          fx += dedr_r * ddx + e2rd * dx;
+          fy += dedr_r * ddy + e2rd * dy;
+          fz += dedr_r * ddz + e2rd * dz;
+          dq += dcq * rd;
+        } else {
+          fx += dedr_r * dx;
+          fy += dedr_r * dy;
+          fz += dedr_r * dz;
+          dq += cq;
+          ex += (double)(kqi * cq);
+        }
       }
     }
     if (vi) {
@@ -380,11 +474,15 @@ __global__ void __launch_bounds__(TileCfg<T>::NW * 32) tile_kernel(TileArgs<T> A
       Acc<T>::add(&A.gx[3 * si + 1], (double)fy);
       Acc<T>::add(&A.gx[3 * si + 2], (double)fz);
       Acc<T>::add(&A.gq[si], (double)kc * (double)dq);
+      if constexpr (MODE != 0) {
+        Acc<T>::add(&A.gs[si], (double)d_sig);
+        Acc<T>::add(&A.ga[si], (double)d_a);
+      }
     }
     // energies: warp sum, then one order-independent accumulation per work item
     ep = warp_sum(ep);
     ex = warp_sum(ex);
-    if (lane == 0) {
+    if (MODE != 2 && lane == 0) {
       Acc<T>::add(&A.energies[2 * isys], 0.5 * ep);
       Acc<T>::add(&A.energies[2 * isys + 1], 0.5 * ex);
     }

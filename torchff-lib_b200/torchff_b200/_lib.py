@@ -90,6 +90,8 @@ _SIGS = {
     "tff_timer_elapsed_ms": (i32, [vp, i32, i32, C.POINTER(C.c_float)]),
     "tff_system_eval_timed": (i32, [vp, vp, vp, vp, vp, vp, vp]),
     "tff_system_kernel_launches": (i32, [vp]),
+    "tff_system_eval_grads": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "tff_system_hvp": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "tff_batch_device_bytes": (sz, [C.POINTER(BatchDesc)]),
     "tff_batch_create": (i32, [C.POINTER(BatchDesc), C.POINTER(vp)]),
     "tff_batch_destroy": (i32, [vp]),
@@ -105,6 +107,7 @@ _SIGS = {
     "tff_server_release": (i32, [vp, i64]),
     "tff_server_drain": (i32, [vp, f64]),
     "tff_server_get_stats": (i32, [vp, C.POINTER(ServerStats)]),
+    "tff_server_hold": (i32, [vp, i32]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

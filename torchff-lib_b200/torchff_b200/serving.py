@@ -142,6 +142,18 @@ class BatchEvaluator:
         return int(v.value)
 
 
+class PreparedRequest:
+    """Contiguous float64 inputs and the C request descriptor of one system."""
+
+    def __init__(self, spec: SystemSpec):
+        self.natoms = spec.natoms
+        self._excl = np.ascontiguousarray(spec.excl_pairs, dtype=np.int64).reshape(-1, 2)
+        self._arrays = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                        (spec.coords, spec.box, spec.charges, spec.sigma, spec.epsilon)]
+        self.desc = _lib.RequestDesc(spec.natoms, int(spec.pme_grid), *(a.ctypes.data for a in self._arrays),
+                                     self._excl.shape[0], self._excl.ctypes.data, None, None)
+
+
 class ServerRequest:
     """Handle of a submitted request; energy / forces are filled in when it completes."""
 
@@ -193,20 +205,28 @@ class Server:
         with torch.cuda.device(self.device):
             check(lib.tff_server_create(C.byref(self.desc), C.byref(self._h)), "tff_server_create")
 
-    def submit(self, spec: SystemSpec) -> ServerRequest:
-        """Queue one system; inputs are copied now, outputs arrive in the returned request."""
-        excl = np.ascontiguousarray(spec.excl_pairs, dtype=np.int64).reshape(-1, 2)
-        arrays = [np.ascontiguousarray(a, dtype=np.float64) for a in
-                  (spec.coords, spec.box, spec.charges, spec.sigma, spec.epsilon)]
+    @staticmethod
+    def prepare(spec: SystemSpec) -> "PreparedRequest":
+        """The request descriptor of a system, built once (submit() accepts it directly)."""
+        return PreparedRequest(spec)
+
+    def submit(self, spec) -> ServerRequest:
+        """Queue one system (a SystemSpec or a PreparedRequest); inputs are copied now,
+        outputs arrive in the returned request."""
+        prep = spec if isinstance(spec, PreparedRequest) else PreparedRequest(spec)
+        out_e = np.empty(1, dtype=np.float64)
+        out_f = np.empty((prep.natoms, 3), dtype=np.float64)
+        d = prep.desc
+        d.energy, d.forces = out_e.ctypes.data, out_f.ctypes.data
         ticket = C.c_int64()
-        out_e = np.zeros(1, dtype=np.float64)
-        out_f = np.zeros((spec.natoms, 3), dtype=np.float64)
-        d = _lib.RequestDesc(spec.natoms, int(spec.pme_grid), *(a.ctypes.data for a in arrays), excl.shape[0],
-                             excl.ctypes.data, out_e.ctypes.data, out_f.ctypes.data)
         check(lib.tff_server_submit(self._h, C.byref(d), C.byref(ticket)), "tff_server_submit")
         req = ServerRequest(self, int(ticket.value), out_e, out_f)
         self._live[req.ticket] = req
         return req
+
+    def hold(self, on: bool = True) -> None:
+        """While held, no new batch starts; requests keep queueing (e.g. to measure a full queue)."""
+        check(lib.tff_server_hold(self._h, 1 if on else 0), "tff_server_hold")
 
     def drain(self, timeout: float | None = None) -> None:
         check(lib.tff_server_drain(self._h, -1.0 if timeout is None else float(timeout)), "tff_server_drain")

@@ -53,6 +53,9 @@ class FixedChargeSystem:
                                             ex.shape[0], ex.ctypes.data_as(ctypes.c_void_p), ctypes.byref(h)),
                     "tff_system_create")
         self._h = h
+        # the parameters the system holds (system dtype), for callers that pass none
+        self.defaults = {k: torch.tensor(v, dtype=dtype, device=self.device) for k, v in
+                         (("charges", q), ("sigma", s), ("epsilon", e))}
 
     @classmethod
     def from_water_box(cls, wb, dtype=torch.float32, device="cuda", **kw):
@@ -117,6 +120,37 @@ class FixedChargeSystem:
                                            ctypes.c_void_p(fp), self._stream()), "tff_system_eval_host")
         return e.value
 
+    def evaluate_grads(self, coords: torch.Tensor, box: torch.Tensor) -> dict:
+        """Energy, forces and first derivatives with respect to the per-atom parameters
+        (dE/dq, dE/dsigma, dE/depsilon; dE/deps_i = 0 where eps_i = 0)."""
+        x = coords.detach().to(self.device, self.dtype).contiguous()
+        b = box.detach().to(self.device, self.dtype).contiguous()
+        n = self.natoms
+        out = {"energy": torch.empty(1, dtype=torch.float64, device=self.device),
+               "forces": torch.empty_like(x)}
+        for k in ("grad_charges", "grad_sigma", "grad_epsilon"):
+            out[k] = torch.empty(n, dtype=self.dtype, device=self.device)
+        L.check(L.lib.tff_system_eval_grads(self._h, L.ptr(x), L.ptr(b), L.ptr(out["energy"]), L.ptr(out["forces"]),
+                                            L.ptr(out["grad_charges"]), L.ptr(out["grad_sigma"]),
+                                            L.ptr(out["grad_epsilon"]), self._stream()), "tff_system_eval_grads")
+        out["energy"] = out["energy"][0]
+        return out
+
+    def hvp(self, coords: torch.Tensor, box: torch.Tensor, direction: torch.Tensor) -> dict:
+        """Derivatives of s = sum_i u_i . dE/dx_i (u = `direction`, (N,3)) with respect to the
+        coordinates, charges, sigma and epsilon: one Hessian-vector product."""
+        x = coords.detach().to(self.device, self.dtype).contiguous()
+        b = box.detach().to(self.device, self.dtype).contiguous()
+        u = direction.detach().to(self.device, self.dtype).contiguous()
+        n = self.natoms
+        out = {"coords": torch.empty_like(x)}
+        for k in ("charges", "sigma", "epsilon"):
+            out[k] = torch.empty(n, dtype=self.dtype, device=self.device)
+        L.check(L.lib.tff_system_hvp(self._h, L.ptr(x), L.ptr(b), L.ptr(u), L.ptr(out["coords"]),
+                                     L.ptr(out["charges"]), L.ptr(out["sigma"]), L.ptr(out["epsilon"]),
+                                     self._stream()), "tff_system_hvp")
+        return out
+
     def status(self) -> int:
         v = ctypes.c_int(0)
         L.check(L.lib.tff_system_status(self._h, self._stream(), ctypes.byref(v)), "tff_system_status")
@@ -169,31 +203,74 @@ class StageTimer:
             self.handle = None
 
 
+class _SystemGradFn(torch.autograd.Function):
+    """(coords, charges, sigma, epsilon) -> (dE/dx, dE/dq, dE/dsigma, dE/deps), values computed
+    by the forward evaluation; its backward is the Hessian-vector product along the
+    cotangent of dE/dx (what a force-matching loss needs)."""
+
+    @staticmethod
+    def forward(ctx, coords, box, q, sig, eps, gx, gq, gs, ge, system):
+        ctx.save_for_backward(coords, box, q, sig, eps)
+        ctx.system = system
+        return gx.clone(), gq.clone(), gs.clone(), ge.clone()
+
+    @staticmethod
+    def backward(ctx, vx, vq, vs, ve):
+        for v in (vq, vs, ve):
+            if v is not None and bool(torch.any(v != 0)):
+                raise NotImplementedError("second derivatives along charge/sigma/epsilon directions are not "
+                                          "implemented; differentiate dE/dx only (force matching)")
+        coords, box, q, sig, eps = ctx.saved_tensors
+        system = ctx.system
+        if vx is None:
+            return (None,) * 10
+        system.set_parameters(q, sig, eps)
+        h = system.hvp(coords, box, vx)
+        cast = lambda t, ref: t.to(ref.dtype)  # noqa: E731
+        return (cast(h["coords"], coords), None, cast(h["charges"], q), cast(h["sigma"], sig),
+                cast(h["epsilon"], eps), None, None, None, None, None)
+
+
 class _SystemEnergyFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, coords, box, charges, system: FixedChargeSystem):
-        out = system.evaluate(coords, box, grad_charges=ctx.needs_input_grad[2])
-        ctx.save_for_backward(out["forces"], out.get("grad_charges"))
+    def forward(ctx, coords, box, q, sig, eps, system: FixedChargeSystem):
+        system.set_parameters(q, sig, eps)
+        if ctx.needs_input_grad[3] or ctx.needs_input_grad[4]:
+            out = system.evaluate_grads(coords, box)
+            gs, ge = out["grad_sigma"], out["grad_epsilon"]
+        else:
+            out = system.evaluate(coords, box, grad_charges=True)
+            gs = ge = torch.zeros(system.natoms, dtype=system.dtype, device=system.device)
+        gx = (-out["forces"]).to(coords.dtype)
+        ctx.save_for_backward(coords, box, q, sig, eps, gx, out["grad_charges"].to(q.dtype), gs.to(sig.dtype),
+                              ge.to(eps.dtype))
+        ctx.system = system
         return out["energy"].to(coords.dtype)
 
     @staticmethod
     def backward(ctx, g):
-        f, gq = ctx.saved_tensors
-        return -f * g, None, (None if gq is None else gq * g), None
+        coords, box, q, sig, eps, gx, gq, gs, ge = ctx.saved_tensors
+        dx, dq, ds, de = _SystemGradFn.apply(coords, box, q, sig, eps, gx, gq, gs, ge, ctx.system)
+        return g * dx, None, g * dq, g * ds, g * de, None
 
 
 class FixedChargeNonbonded(nn.Module):
-    """nn.Module view of a FixedChargeSystem: ``forward(coords, box) -> E`` with forces via autograd.
+    """nn.Module view of a FixedChargeSystem: ``forward(coords, box, charges, sigma, epsilon) -> E``.
 
-    ``charges`` passed to forward (optional) must equal the system's charges; it is
-    accepted so that dE/dq flows to a leaf tensor.
+    Forces and parameter gradients come from autograd, and the backward is itself
+    differentiable along dE/dx: a loss on the forces (force matching) back-propagates to
+    coordinates, charges, sigma and epsilon through one Hessian-vector product. Parameters
+    left as None are the system's own.
     """
 
     def __init__(self, system: FixedChargeSystem):
         super().__init__()
         self.system = system
 
-    def forward(self, coords: torch.Tensor, box: torch.Tensor, charges: torch.Tensor | None = None):
-        if charges is not None:
-            self.system.set_parameters(charges=charges)
-        return _SystemEnergyFn.apply(coords, box, charges, self.system)
+    def forward(self, coords: torch.Tensor, box: torch.Tensor, charges: torch.Tensor | None = None,
+                sigma: torch.Tensor | None = None, epsilon: torch.Tensor | None = None):
+        d = self.system.defaults
+        q = d["charges"] if charges is None else charges
+        s = d["sigma"] if sigma is None else sigma
+        e = d["epsilon"] if epsilon is None else epsilon
+        return _SystemEnergyFn.apply(coords, box, q, s, e, self.system)

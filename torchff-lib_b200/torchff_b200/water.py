@@ -183,3 +183,13 @@ def perturbed_frames(wb: WaterBox, n_frames: int, sigma: float, seed: int) -> np
     if n_frames > 1:
         frames[1:] += rng.normal(0.0, sigma, size=frames[1:].shape)
     return frames
+
+
+def force_matching_parameters(wb: WaterBox, seed: int, noise: float = 0.05) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Per-atom (charges, sigma, epsilon) for force matching: TIP3P charges with seeded
+    uniform +-`noise` relative noise, shifted back to a neutral total; sigma and epsilon
+    are the TIP3P per-atom values."""
+    rng = np.random.default_rng(seed)
+    q = wb.charges * (1.0 + rng.uniform(-noise, noise, wb.natoms))
+    q -= q.mean()
+    return q, wb.sigma.copy(), wb.epsilon.copy()
