@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section of the water3000 line")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 timing of the water3000 line")
     ap.add_argument("--serving-requests", type=int, default=4096)
+    ap.add_argument("--no-force-matching", action="store_true", help="skip the force-matching section")
     return ap.parse_args()
 
 
@@ -222,6 +223,65 @@ def time_graph_evals(wb, dtype, device, steps: int, warmup: int) -> dict:
     del graph
     return {"value": round(steps / (total / 1e3), 2), "unit": "evals/s", "ms_per_step": round(total / steps, 5),
             "steps": steps, "warmup": warmup}
+
+
+def run_force_matching(device, dtype, rank: int, world: int, frames: int = 16, steps: int = 10,
+                       warmup: int = 3) -> dict:
+    """One force-matching training step = for each of `frames` perturbed frames of the
+    3000-water box: energy, forces (create_graph) and the loss mean |F - F_target|^2; then
+    backward to the per-atom charges, sigma and epsilon (double backward). Frames are split
+    over the ranks; the parameter gradients are summed over ranks with one all-reduce."""
+    import numpy as np
+    import torch
+
+    from torchff_b200.distributed import allreduce_sum_, frame_shard, max_over_ranks
+    from torchff_b200.system import FixedChargeNonbonded, FixedChargeSystem
+    from torchff_b200.water import force_matching_parameters, perturbed_frames, water_box_3000
+
+    wb = water_box_3000()
+    q0, s0, e0 = force_matching_parameters(wb, seed=0)
+    xs = perturbed_frames(wb, frames, 0.005, seed=1)
+    targets = np.random.default_rng(2).normal(0.0, 300.0, size=xs.shape)
+    mine = frame_shard(frames, rank, world)
+    sysm = FixedChargeSystem(q0, s0, e0, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid, dtype=dtype,
+                             device=device)
+    model = FixedChargeNonbonded(sysm)
+    box = torch.tensor(wb.box, dtype=dtype, device=device)
+    X = [torch.tensor(xs[f], dtype=dtype, device=device, requires_grad=True) for f in mine]
+    T = [torch.tensor(targets[f], dtype=dtype, device=device) for f in mine]
+    params = [torch.tensor(a, dtype=dtype, device=device, requires_grad=True) for a in (q0, s0, e0)]
+
+    def step():
+        for p in params:
+            p.grad = None
+        total = torch.zeros((), dtype=torch.float64, device=device)
+        for x, t in zip(X, T):
+            E = model(x, box, *params)
+            (gx,) = torch.autograd.grad(E, x, create_graph=True)
+            loss = torch.mean((-gx - t) ** 2) / frames
+            loss.backward()
+            total += loss.detach().double()
+        allreduce_sum_([p.grad for p in params] + [total])
+        return total
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize(device)
+    if world > 1:
+        dist.barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        step()
+    end.record()
+    end.synchronize()
+    ms = max_over_ranks(start.elapsed_time(end) / steps, device)
+    return {"workload": "3000-water box, per-atom q (+-5% noise, neutral), sigma, eps leaves; "
+                        f"{frames} frames with N(0, 0.005 nm) coordinate noise; loss mean |F - F_target|^2",
+            "precision": "mixed" if dtype == torch.float32 else "fp64", "frames": frames, "ranks": world,
+            "ms_per_step": round(ms, 3), "frames_per_s": round(frames / (ms / 1e3), 1),
+            "per_frame": "forward with parameter gradients + one Hessian-vector product (double backward)",
+            "gradient_allreduce": "NCCL sum of dE/d(q, sigma, eps) over ranks" if world > 1 else None}
 
 
 def run_serving(device, n_requests: int = 4096, seed: int = 0) -> dict:
@@ -442,6 +502,9 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * args.e2e_steps / (float(te.item()) / 1e3)
+    fm = None
+    if not args.no_force_matching and args.workload == "water3000":
+        fm = [run_force_matching(device, torch.float64, rank, world), run_force_matching(device, torch.float32, rank, world)]
     h2d = wb.natoms * 3 * 8 + 9 * 8
     d2h = wb.natoms * 3 * 8 + 8
 
@@ -498,6 +561,8 @@ def run_ours(args):
             },
             "clocks": clk,
         }
+        if fm is not None:
+            result["force_matching"] = fm
         if world == 1 and not args.no_fp64 and dtype == torch.float32:
             result["fp64"] = time_graph_evals(wb, torch.float64, device, min(args.steps, 500), args.warmup)
         if world == 1 and not args.no_serving:

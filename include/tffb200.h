@@ -272,7 +272,10 @@ int tff_system_kernel_launches(tff_system sys);
  * system's result is the one a single-system evaluation of the same dtype gives (mixed
  * precision: bit-identical whatever else is in the batch). Same physics as tff_system_*;
  * cutoff, Ewald alpha and the Coulomb constant are shared by the batch.
- * Per system: 1 <= natoms <= 16384, 6 <= K <= 128.
+ * Per system: 1 <= natoms <= 16384, 6 <= K <= 96 (TFF_F32) or 64 (TFF_F64). The
+ * reciprocal-space transforms of a batch are a direct 3-D DFT of every grid (one launch per
+ * axis pass for all sizes), not cuFFT; results match the single-system (cuFFT) path to FP
+ * rounding.
  * --------------------------------------------------------------------------- */
 typedef struct tff_batch_s *tff_batch;
 
@@ -331,7 +334,7 @@ typedef struct tff_server_desc {
 
 typedef struct tff_request {
   int64_t natoms;               /* 1..16384 */
-  int pme_grid;                 /* K, 6..128 */
+  int pme_grid;                 /* K, 6..96 (TFF_F32) or 6..64 (TFF_F64) */
   const double *coords;         /* host (natoms, 3) */
   const double *box;            /* host (3, 3), rows are box vectors */
   const double *charges;        /* host (natoms) */

@@ -1,11 +1,12 @@
 """Batched evaluation (tff_batch) and the continuous-batching server (tff_server).
 
 Each system of a batch must give the single-system result. The cluster lists and the
-fixed-point real-space sums are the same whatever else is in the batch; the reciprocal
-part differs only by the FP32 rounding of cuFFT, which runs the grids of equal size as one
-batched transform (a grid's rounding can depend on the batch count of its plan).
-Tolerances for "same system, other company": energy 1e-9 relative, forces 1e-6 of the
-largest force component.
+fixed-point real-space sums are the same; the reciprocal part of a batch uses a direct DFT
+where the single-system path uses cuFFT, so the two agree to FP32 transform rounding:
+energy within 1e-8 of the summed magnitudes of the energy terms (the total is a
+near-cancelling sum), forces 1e-6 of the largest component. Within the batched path the
+summation order of every reduction and transform depends on the system alone, so a
+system's result alone and in a mix agree to 1e-9 (energy, relative) and 1e-6 (forces).
 FP64 batches match the FP64 oracle to 1e-10 (energy) and 1e-8 (forces). The request sizes
 include boxes shorter than twice the cutoff (64 and 150 waters), evaluated with the
 minimum-image convention like the single-system path and the oracle.
@@ -35,7 +36,7 @@ def _single(wb, dtype):
     from torchff_b200.system import FixedChargeSystem
 
     s = FixedChargeSystem.from_water_box(wb, dtype=dtype)
-    return s.evaluate(t(wb.coords, dtype), t(wb.box, dtype))
+    return s.evaluate(t(wb.coords, dtype), t(wb.box, dtype), terms=True)
 
 
 def _evaluator(dtype, wbs):
@@ -57,7 +58,8 @@ def test_batch_matches_single_system_mixed(mixed_boxes):
     assert ev.status() == 0
     for k, wb in enumerate(wbs):
         ref = _single(wb, torch.float32)
-        assert rel(e[k].item(), ref["energy"].item()) < 1e-9, wb.n_waters
+        scale = float(ref["terms"].abs().sum())
+        assert abs(e[k].item() - ref["energy"].item()) < 1e-8 * scale, wb.n_waters
         assert rel_max(f[k], ref["forces"]) < 1e-6, wb.n_waters
 
 

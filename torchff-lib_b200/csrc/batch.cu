@@ -4,20 +4,18 @@
 //   main stream : batch_sort (one block per system: its own box facts and Hilbert cell
 //                 grid) -> cluster bounds -> cluster neighbours -> sorted parameters ->
 //                 tile kernel -> [join] -> finalize (forces, one energy per system)
-//   PME stream  : spread (blockIdx.y = system) -> [fixed point -> FP32] -> R2C FFT per
-//                 group of equal K -> convolution -> C2R FFT per group -> gather
+//   PME stream  : spread (blockIdx.y = system) -> [fixed point -> FP32] -> 3-D real DFT
+//                 (three axis passes over all systems) -> convolution -> inverse DFT
+//                 (three passes) -> gather
 //
 // Systems are laid out one after another in every array; the cluster lists never leave a
 // system, and every per-system reduction runs over a block count that depends on that
 // system alone, so a system's result does not depend on what else is in the batch. The
-// PME grids are ordered by K so that each group of equal K is one batched cuFFT call (the
-// group is split into power-of-two counts, whose plans are cached).
+// reciprocal-space transforms are the batched direct DFT of pme.cuh (one launch per axis
+// pass for all grid sizes): cuFFT transforms grids of one size per plan, and a batch of
+// a few hundred sizes would need hundreds of plans and launches per evaluation.
 #include <algorithm>
 #include <cmath>
-#include <map>
-#include <mutex>
-#include <numeric>
-#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -26,7 +24,9 @@
 namespace tff {
 namespace {
 
-constexpr int kBatchMaxK = 128;
+// Largest PME grid side of a batch: the DFT stages two K x K planes in shared memory.
+constexpr int kBatchMaxK = 96;
+constexpr int kBatchMaxK64 = 64;
 
 // Grid distances inside the batch: every real grid starts on a 256-byte boundary and every
 // complex grid on a 256-byte (FP32) boundary, as cuFFT wants aligned transform inputs.
@@ -99,57 +99,6 @@ inline BatchLayout batch_layout(int dtype, int64_t max_atoms, int64_t max_system
   return L;
 }
 
-struct FftGroup {
-  int K;
-  int64_t grid_off, cplx_off;
-  int count;
-};
-
-// Batched cuFFT plans of the process, shared by every batch object: (device, dtype, K,
-// count) -> (R2C, C2R, work bytes). Plans run without their own work area; each batch
-// object passes its own, so batches on different streams can use one plan concurrently.
-struct PlanEntry {
-  cufftHandle r2c, c2r;
-  size_t work;
-};
-std::mutex g_plan_mu;
-std::map<std::tuple<int, int, int, int>, PlanEntry> g_plans;
-
-int shared_plans(int dtype, int K, int count, PlanEntry &out) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  const auto key = std::make_tuple(dev, dtype, K, count);
-  std::lock_guard<std::mutex> g(g_plan_mu);
-  auto it = g_plans.find(key);
-  if (it != g_plans.end()) {
-    out = it->second;
-    return TFF_OK;
-  }
-  const bool f64 = dtype == TFF_F64;
-  int n[3] = {K, K, K}, cn[3] = {K, K, K / 2 + 1};
-  const int rd = (int)real_dist(K), cd = (int)cplx_dist(K);
-  cufftHandle h[2] = {0, 0};
-  size_t work[2] = {0, 0};
-  for (int d = 0; d < 2; ++d) {
-    cufftResult r = cufftCreate(&h[d]);
-    if (r == CUFFT_SUCCESS) r = cufftSetAutoAllocation(h[d], 0);
-    if (r == CUFFT_SUCCESS) {
-      if (d == 0)
-        r = cufftMakePlanMany(h[d], 3, n, n, 1, rd, cn, 1, cd, f64 ? CUFFT_D2Z : CUFFT_R2C, count, &work[d]);
-      else
-        r = cufftMakePlanMany(h[d], 3, n, cn, 1, cd, n, 1, rd, f64 ? CUFFT_Z2D : CUFFT_C2R, count, &work[d]);
-    }
-    if (r != CUFFT_SUCCESS) {
-      for (int e = 0; e <= d; ++e)
-        if (h[e]) cufftDestroy(h[e]);
-      return pme_cufft_fail(r, "batched plan");
-    }
-  }
-  out = PlanEntry{h[0], h[1], std::max(work[0], work[1])};
-  g_plans[key] = out;
-  return TFF_OK;
-}
-
 }  // namespace
 }  // namespace tff
 
@@ -163,10 +112,7 @@ struct tff_batch_s {
   cudaEvent_t table_ev = nullptr;  // the table upload of the previous evaluation
   cudaStream_t pme_stream = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
-  void *fft_work = nullptr;        // this batch's cuFFT work area
-  size_t fft_work_bytes = 0;
   std::vector<BatchSys> host_sys;
-  std::vector<FftGroup> groups;
   int device = 0;
 };
 
@@ -175,7 +121,6 @@ namespace {
 
 void free_batch(tff_batch b) {
   if (!b) return;
-  if (b->fft_work) cudaFree(b->fft_work);
   if (b->ws) cudaFree(b->ws);
   if (b->table) cudaFreeHost(b->table);
   if (b->table_ev) cudaEventDestroy(b->table_ev);
@@ -185,57 +130,26 @@ void free_batch(tff_batch b) {
   delete b;
 }
 
-// Plans for `count` contiguous K^3 grids (created on first use, process-wide) with this
-// batch's work area grown to fit; growing waits for the batch's own streams.
-int get_plans(tff_batch b, int K, int count, cufftHandle &r2c, cufftHandle &c2r) {
-  PlanEntry p;
-  int st = shared_plans(b->desc.dtype, K, count, p);
-  if (st != TFF_OK) return st;
-  const size_t need = std::max<size_t>(256, p.work);
-  if (need > b->fft_work_bytes) {
-    TFF_CUDA(cudaStreamSynchronize(b->pme_stream));
-    if (b->fft_work) TFF_CUDA(cudaFree(b->fft_work));
-    b->fft_work = nullptr;
-    b->fft_work_bytes = 0;
-    TFF_CUDA(cudaMalloc(&b->fft_work, need));
-    b->fft_work_bytes = need;
-  }
-  r2c = p.r2c;
-  c2r = p.c2r;
-  return TFF_OK;
-}
-
-// One FFT direction over every group; a group of count c runs as the binary digits of c.
+// One direction of the 3-D real DFT of every grid of the batch (three axis passes).
 template <class T>
-int run_ffts(tff_batch b, bool forward, T *real, typename CplxOf<T>::type *cplx, cudaStream_t s) {
-  for (const FftGroup &g : b->groups) {
-    int64_t goff = g.grid_off, coff = g.cplx_off;
-    const int64_t rstep = real_dist(g.K), cstep = cplx_dist(g.K);
-    for (int bit = 30; bit >= 0; --bit) {
-      const int cnt = 1 << bit;
-      if (!(g.count & cnt)) continue;
-      cufftHandle r2c, c2r;
-      int st = get_plans(b, g.K, cnt, r2c, c2r);
-      if (st != TFF_OK) return st;
-      cufftHandle h = forward ? r2c : c2r;
-      // stream, work area and launch of a shared plan in one critical section
-      std::lock_guard<std::mutex> guard(g_plan_mu);
-      cufftResult r = cufftSetStream(h, s);
-      if (r == CUFFT_SUCCESS) r = cufftSetWorkArea(h, b->fft_work);
-      if (r != CUFFT_SUCCESS) return pme_cufft_fail(r, "cufftSetStream/WorkArea");
-      if (sizeof(T) == 4) {
-        r = forward ? cufftExecR2C(h, reinterpret_cast<cufftReal *>(real + goff), reinterpret_cast<cufftComplex *>(cplx + coff))
-                    : cufftExecC2R(h, reinterpret_cast<cufftComplex *>(cplx + coff), reinterpret_cast<cufftReal *>(real + goff));
-      } else {
-        r = forward ? cufftExecD2Z(h, reinterpret_cast<cufftDoubleReal *>(real + goff),
-                                   reinterpret_cast<cufftDoubleComplex *>(cplx + coff))
-                    : cufftExecZ2D(h, reinterpret_cast<cufftDoubleComplex *>(cplx + coff),
-                                   reinterpret_cast<cufftDoubleReal *>(real + goff));
-      }
-      if (r != CUFFT_SUCCESS) return pme_cufft_fail(r, forward ? "batched forward FFT" : "batched inverse FFT");
-      goff += cnt * rstep;
-      coff += cnt * cstep;
-    }
+int run_dft(const BatchSys *dsys, int nsys, int kmax, bool forward, T *real, typename CplxOf<T>::type *cplx,
+            cudaStream_t s) {
+  const dim3 grid((unsigned)kmax, (unsigned)nsys);
+  const size_t smem = batch_dft_smem<T>(kmax);
+  if (forward) {
+    batch_dft_kernel<T, kDftZR2C><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
+    TFF_LAUNCHED();
+    batch_dft_kernel<T, kDftY><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
+    TFF_LAUNCHED();
+    batch_dft_kernel<T, kDftX><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
+    TFF_LAUNCHED();
+  } else {
+    batch_dft_kernel<T, kDftXInv><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
+    TFF_LAUNCHED();
+    batch_dft_kernel<T, kDftYInv><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
+    TFF_LAUNCHED();
+    batch_dft_kernel<T, kDftZC2R><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
+    TFF_LAUNCHED();
   }
   return TFF_OK;
 }
@@ -254,7 +168,8 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
     const int64_t n = natoms[i];
     const int K = pme_grid[i];
     TFF_ARG(n >= 1 && n <= kBatchMaxAtoms, "system %d: natoms %lld outside [1, %d]", i, (long long)n, kBatchMaxAtoms);
-    TFF_ARG(K >= 6 && K <= kBatchMaxK, "system %d: PME grid %d outside [6, %d]", i, K, kBatchMaxK);
+    const int kmax_dtype = sizeof(T) == 8 ? kBatchMaxK64 : kBatchMaxK;
+    TFF_ARG(K >= 6 && K <= kmax_dtype, "system %d: PME grid %d outside [6, %d]", i, K, kmax_dtype);
     BatchSys &y = hs[i];
     y.atom_off = ao;
     y.natoms = n;
@@ -274,18 +189,13 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
     so += y.nsup;
   }
   TFF_ARG(ao <= L.atoms, "batch holds %lld atoms; capacity %lld", (long long)ao, (long long)L.atoms);
-  std::vector<int> order(nsys);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return hs[a].K < hs[c].K; });
-  b->groups.clear();
-  for (int i : order) {
-    BatchSys &y = hs[i];
+  int kmax = 6;
+  for (BatchSys &y : hs) {
     y.grid_off = go;
     y.cplx_off = xo;
-    if (b->groups.empty() || b->groups.back().K != y.K) b->groups.push_back(FftGroup{y.K, go, xo, 0});
-    b->groups.back().count++;
     go += real_dist(y.K);
     xo += cplx_dist(y.K);
+    kmax = std::max(kmax, y.K);
   }
   TFF_ARG(go <= L.grid + 64 * L.systems, "batch holds %lld PME grid points; capacity %lld", (long long)go,
           (long long)L.grid);
@@ -355,13 +265,13 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
     real = reinterpret_cast<T *>(fix);
   }
   auto *cplx = reinterpret_cast<typename CplxOf<T>::type *>(w + L.cplx);
-  int st = run_ffts<T>(b, true, real, cplx, ps);
+  int st = run_dft<T>(dsys, nsys, kmax, true, real, cplx, ps);
   if (st != TFF_OK) return st;
   batch_convolve_kernel<T><<<pgrid, kPmeBlock, 0, ps>>>(dsys, cplx, boxes, b->desc.ewald_alpha,
                                                         reinterpret_cast<const T *>(w + L.moduli), partials, tickets,
                                                         e_pme);
   TFF_LAUNCHED();
-  if ((st = run_ffts<T>(b, false, real, cplx, ps)) != TFF_OK) return st;
+  if ((st = run_dft<T>(dsys, nsys, kmax, false, real, cplx, ps)) != TFF_OK) return st;
   batch_gather_kernel<T><<<pgrid, kPmeBlock, 0, ps>>>(dsys, x, q, boxes, real, b->desc.ewald_alpha, pme_phi, pme_grad,
                                                       partials, tickets, e_pme);
   TFF_LAUNCHED();
@@ -415,6 +325,13 @@ template <class T>
 int set_sort_smem() {
   TFF_CUDA(cudaFuncSetAttribute(batch_sort_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)kBatchSortSmem));
+  const int dft = (int)batch_dft_smem<T>(sizeof(T) == 8 ? kBatchMaxK64 : kBatchMaxK);
+  TFF_CUDA(cudaFuncSetAttribute(batch_dft_kernel<T, kDftZR2C>, cudaFuncAttributeMaxDynamicSharedMemorySize, dft));
+  TFF_CUDA(cudaFuncSetAttribute(batch_dft_kernel<T, kDftY>, cudaFuncAttributeMaxDynamicSharedMemorySize, dft));
+  TFF_CUDA(cudaFuncSetAttribute(batch_dft_kernel<T, kDftX>, cudaFuncAttributeMaxDynamicSharedMemorySize, dft));
+  TFF_CUDA(cudaFuncSetAttribute(batch_dft_kernel<T, kDftXInv>, cudaFuncAttributeMaxDynamicSharedMemorySize, dft));
+  TFF_CUDA(cudaFuncSetAttribute(batch_dft_kernel<T, kDftYInv>, cudaFuncAttributeMaxDynamicSharedMemorySize, dft));
+  TFF_CUDA(cudaFuncSetAttribute(batch_dft_kernel<T, kDftZC2R>, cudaFuncAttributeMaxDynamicSharedMemorySize, dft));
   return TFF_OK;
 }
 
@@ -514,8 +431,9 @@ int tff_batch_status(tff_batch b, tff_stream_t stream, int *status) {
 
 int tff_batch_kernel_launches(tff_batch b) {
   if (!b) return 0;
-  // sort, bounds, neighbours, params, tile, finalize; spread, [to_real], convolve, gather
-  return 6 + (b->desc.dtype == TFF_F32 ? 4 : 3);
+  // sort, bounds, neighbours, params, tile, finalize; spread, [to_real], 3 DFT passes,
+  // convolve, 3 inverse passes, gather
+  return 6 + (b->desc.dtype == TFF_F32 ? 10 : 9);
 }
 
 }  // extern "C"

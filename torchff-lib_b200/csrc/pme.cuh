@@ -428,6 +428,125 @@ __global__ void __launch_bounds__(kPmeBlock) pme_gather_hvp_kernel(PlainAtoms<T>
   }
 }
 
+// ---- batched 3-D real DFT of many grids of different sizes (the serving path)
+// One launch per axis pass over every system of a batch: blockIdx.y = system, blockIdx.x =
+// plane (0..K-1). A block stages one plane in shared memory as `lines` x `points` with an
+// odd row stride (so lanes reading one point of consecutive lines hit distinct banks),
+// evaluates each output as a direct sum over the line with a twiddle table
+// w[m] = exp(-+2 pi i m / K) (consecutive lanes share the twiddle: a broadcast), stages
+// the outputs and writes them back contiguously. Layouts are those of cuFFT's R2C/C2R:
+// real grid [x][y][z] (K^3), half spectrum [kx][ky][kz] (K x K x (K/2+1)), the inverse
+// unnormalised. The summation order is fixed, so a grid's result does not depend on the
+// batch it runs in.
+enum BatchDftPass { kDftZR2C = 0, kDftY, kDftX, kDftXInv, kDftYInv, kDftZC2R };
+constexpr int kDftThreads = 256;
+
+__host__ __device__ inline int dft_stride(int K) { return K | 1; }
+
+// Shared memory of one block of a pass for grid side K (twiddles + input + output planes).
+template <class T>
+inline size_t batch_dft_smem(int K) {
+  return (size_t)(K + 2 * (size_t)K * dft_stride(K)) * 2 * sizeof(T);
+}
+
+template <class T, int PASS>
+__global__ void __launch_bounds__(kDftThreads) batch_dft_kernel(const BatchSys *sys, T *real,
+                                                                typename CplxOf<T>::type *cplx) {
+  using C = typename CplxOf<T>::type;
+  const BatchSys &b = sys[blockIdx.y];
+  const int K = b.K;
+  if ((int)blockIdx.x >= K) return;
+  const int Kz = K / 2 + 1, st = dft_stride(K), p = blockIdx.x;
+  constexpr bool kInverse = PASS >= kDftXInv;
+  extern __shared__ __align__(16) unsigned char dft_smem[];
+  C *tw = reinterpret_cast<C *>(dft_smem);
+  C *in = tw + K;
+  C *out = in + (size_t)K * st;
+  for (int m = threadIdx.x; m < K; m += blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * m / K, &sn, &cs);
+    tw[m].x = (T)cs;
+    tw[m].y = (T)(kInverse ? sn : -sn);
+  }
+  // plane geometry: lines x points in, lines x nout out
+  const int lines = (PASS == kDftZR2C || PASS == kDftZC2R) ? K : Kz;
+  const int points = PASS == kDftZC2R ? Kz : K;
+  const int nout = PASS == kDftZR2C ? Kz : K;
+  T *rgrid = real + b.grid_off;
+  C *cgrid = cplx + b.cplx_off;
+  // load (global-contiguous order)
+  for (int e = threadIdx.x; e < lines * points; e += blockDim.x) {
+    int line, pt;
+    C v;
+    if (PASS == kDftZR2C) {  // plane x: [y][z] reals
+      line = e / K;
+      pt = e % K;
+      v.x = rgrid[(int64_t)p * K * K + e];
+      v.y = T(0);
+    } else if (PASS == kDftZC2R) {  // plane x: [y][kz]
+      line = e / Kz;
+      pt = e % Kz;
+      v = cgrid[(int64_t)p * K * Kz + e];
+    } else if (PASS == kDftY || PASS == kDftYInv) {  // plane x: [y][kz], lines = kz
+      pt = e / Kz;
+      line = e % Kz;
+      v = cgrid[(int64_t)p * K * Kz + e];
+    } else {  // plane ky: [x][ky][kz], lines = kz
+      pt = e / Kz;
+      line = e % Kz;
+      v = cgrid[((int64_t)pt * K + p) * Kz + line];
+    }
+    in[line * st + pt] = v;
+  }
+  __syncthreads();
+  // outputs: lane-consecutive lines, one frequency (or z) per output
+  for (int o = threadIdx.x; o < lines * nout; o += blockDim.x) {
+    const int line = o % lines, f = o / lines;
+    const C *row = in + line * st;
+    C acc;
+    acc.x = T(0);
+    acc.y = T(0);
+    if (PASS == kDftZC2R) {
+      // real output of a Hermitian half spectrum: T0 + 2 sum_{0<k<K/2} Re(Tk w^(zk)) [+ T_{K/2} (-1)^z]
+      const int kh = (K - 1) / 2;
+      T sum = row[0].x;
+      int idx = 0;
+      for (int k = 1; k <= kh; ++k) {
+        idx += f;
+        if (idx >= K) idx -= K;
+        const C a = row[k], w = tw[idx];
+        sum += T(2) * (a.x * w.x - a.y * w.y);
+      }
+      if (!(K & 1)) sum += (f & 1) ? -row[K / 2].x : row[K / 2].x;
+      acc.x = sum;
+    } else {
+      int idx = 0;
+      for (int j = 0; j < points; ++j) {
+        const C a = row[j], w = tw[idx];
+        acc.x += a.x * w.x - a.y * w.y;
+        acc.y += a.x * w.y + a.y * w.x;
+        idx += f;
+        if (idx >= K) idx -= K;
+      }
+    }
+    out[line * st + f] = acc;
+  }
+  __syncthreads();
+  // store (global-contiguous order)
+  for (int e = threadIdx.x; e < lines * nout; e += blockDim.x) {
+    if (PASS == kDftZR2C) {  // [y][kz]
+      cgrid[(int64_t)p * K * Kz + e] = out[(e / Kz) * st + e % Kz];
+    } else if (PASS == kDftZC2R) {  // [y][z] reals
+      rgrid[(int64_t)p * K * K + e] = out[(e / K) * st + e % K].x;
+    } else if (PASS == kDftY || PASS == kDftYInv) {  // [ky][kz], lines = kz
+      cgrid[(int64_t)p * K * Kz + e] = out[(e % Kz) * st + e / Kz];
+    } else {  // [kx][ky][kz], lines = kz
+      const int f = e / Kz, line = e % Kz;
+      cgrid[((int64_t)f * K + p) * Kz + line] = out[line * st + f];
+    }
+  }
+}
+
 // ---- batched PME: blockIdx.y is the system, blocks [0, BatchSys::pme_blocks) of it work
 // (a count that depends on the system alone, so that its reductions sum in the same order
 // whatever else is in the batch).

@@ -127,7 +127,7 @@ tff_batch_desc lane_batch_desc(const tff_server_desc &d, int64_t atoms, int64_t 
 
 // Device bytes of one lane holding `atoms` atoms (grid capacity in proportion).
 size_t lane_device_bytes(const tff_server_desc &d, int64_t atoms, size_t ts) {
-  const int64_t grid = (int64_t)(atoms * d.grid_points_per_atom) + 128 * 128 * 128;
+  const int64_t grid = (int64_t)(atoms * d.grid_points_per_atom) + 96 * 96 * 96;
   Lane l;
   l.max_atoms = atoms;
   l.max_systems = d.max_systems_per_batch;
@@ -340,7 +340,7 @@ int tff_server_create(const tff_server_desc *desc, tff_server *out) {
   s->lanes.resize(desc->lanes);
   for (Lane &l : s->lanes) {
     l.max_atoms = lo;
-    l.max_grid = (int64_t)(lo * desc->grid_points_per_atom) + 128 * 128 * 128;
+    l.max_grid = (int64_t)(lo * desc->grid_points_per_atom) + 96 * 96 * 96;
     l.max_systems = desc->max_systems_per_batch;
     lane_offsets(l, s->ts);
     tff_batch_desc bd = lane_batch_desc(*desc, l.max_atoms, l.max_grid);
@@ -375,7 +375,8 @@ int tff_server_submit(tff_server s, const tff_request *req, int64_t *ticket) {
   TFF_ARG(s != nullptr && req != nullptr && ticket != nullptr, "server/request/ticket is NULL");
   const int64_t n = req->natoms;
   TFF_ARG(n >= 1 && n <= 16384, "natoms %lld outside [1, 16384]", (long long)n);
-  TFF_ARG(req->pme_grid >= 6 && req->pme_grid <= 128, "pme_grid %d outside [6, 128]", req->pme_grid);
+  const int kmax = s->desc.dtype == TFF_F64 ? 64 : 96;
+  TFF_ARG(req->pme_grid >= 6 && req->pme_grid <= kmax, "pme_grid %d outside [6, %d]", req->pme_grid, kmax);
   TFF_ARG(req->coords && req->box && req->charges && req->sigma && req->epsilon, "NULL input array");
   TFF_ARG(req->nexcl == 0 || req->excl_pairs != nullptr, "exclusion pairs are NULL");
   auto *r = new ServerReq();
