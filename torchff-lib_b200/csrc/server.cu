@@ -136,25 +136,88 @@ size_t lane_device_bytes(const tff_server_desc &d, int64_t atoms, size_t ts) {
   return tff_batch_device_bytes(&bd) + l.in_bytes + l.out_bytes;
 }
 
-int launch_lane(tff_server s, Lane &l) {
-  const size_t ts = s->ts;
-  const int nsys = (int)l.reqs.size();
-  l.natoms.resize(nsys);
-  l.K.resize(nsys);
-  int64_t ao = 0;
-  for (int i = 0; i < nsys; ++i) {
+// Results of requests [i0, i1) of a finished lane into their host buffers.
+void unpack_requests(const Lane &l, size_t ts, const std::vector<int64_t> &off, int i0, int i1) {
+  const double *e = reinterpret_cast<const double *>(l.h_out);
+  for (int i = i0; i < i1; ++i) {
     ServerReq *r = l.reqs[i];
-    const int64_t n = r->n;
+    const int64_t ao = off[i];
+    if (r->energy_out) *r->energy_out = e[i];
+    if (r->forces_out) {
+      const int64_t m = 3 * r->n;
+      if (ts == 8) {
+        std::memcpy(r->forces_out, l.h_out + l.o_f + 3 * ao * 8, m * 8);
+      } else {
+        const float *f = reinterpret_cast<const float *>(l.h_out + l.o_f) + 3 * ao;
+        for (int64_t k = 0; k < m; ++k) r->forces_out[k] = f[k];
+      }
+    }
+  }
+}
+
+// Runs fn(i0, i1) over the requests of a lane, split over up to 4 threads for large batches.
+template <class F>
+void over_requests(const Lane &l, const std::vector<int64_t> &off, F fn) {
+  const int nsys = (int)l.reqs.size();
+  const int64_t ao = off[nsys];
+  const int nthr = ao >= 65536 ? std::min(4, std::max(1, (int)std::thread::hardware_concurrency() / 2)) : 1;
+  if (nthr <= 1) {
+    fn(0, nsys);
+    return;
+  }
+  std::vector<std::thread> pool;
+  int i0 = 0;
+  for (int t = 0; t < nthr; ++t) {
+    const int64_t goal = ao * (t + 1) / nthr;
+    int i1 = i0;
+    while (i1 < nsys && (t == nthr - 1 || off[i1] < goal)) ++i1;
+    pool.emplace_back(fn, i0, i1);
+    i0 = i1;
+  }
+  for (auto &th : pool) th.join();
+}
+
+std::vector<int64_t> atom_offsets(const Lane &l) {
+  std::vector<int64_t> off(l.reqs.size() + 1, 0);
+  for (size_t i = 0; i < l.reqs.size(); ++i) off[i + 1] = off[i] + l.reqs[i]->n;
+  return off;
+}
+
+// Results of a finished lane into the requests' host buffers (worker thread, no lock).
+void unpack_lane(tff_server s, Lane &l) {
+  const std::vector<int64_t> off = atom_offsets(l);
+  const size_t ts = s->ts;
+  over_requests(l, off, [&](int i0, int i1) { unpack_requests(l, ts, off, i0, i1); });
+}
+
+// Copies requests [i0, i1) of a lane into its pinned staging buffer (atom offsets in off).
+void pack_requests(const Lane &l, size_t ts, const std::vector<int64_t> &off, int i0, int i1) {
+  for (int i = i0; i < i1; ++i) {
+    const ServerReq *r = l.reqs[i];
+    const int64_t n = r->n, ao = off[i];
     std::memcpy(l.h_in + l.o_x + 3 * ao * ts, r->coords.data(), 3 * n * ts);
     std::memcpy(l.h_in + l.o_q + ao * ts, r->params.data(), n * ts);
     std::memcpy(l.h_in + l.o_s + ao * ts, r->params.data() + n * ts, n * ts);
     std::memcpy(l.h_in + l.o_e + ao * ts, r->params.data() + 2 * n * ts, n * ts);
     std::memcpy(l.h_in + l.o_box + 9 * (size_t)i * ts, r->box.data(), 9 * ts);
     std::memcpy(l.h_in + l.o_excl + kExclSlots * ao * sizeof(int), r->excl.data(), kExclSlots * n * sizeof(int));
-    l.natoms[i] = n;
-    l.K[i] = r->K;
-    ao += n;
   }
+}
+
+int launch_lane(tff_server s, Lane &l) {
+  const size_t ts = s->ts;
+  const int nsys = (int)l.reqs.size();
+  l.natoms.resize(nsys);
+  l.K.resize(nsys);
+  for (int i = 0; i < nsys; ++i) {
+    l.natoms[i] = l.reqs[i]->n;
+    l.K[i] = l.reqs[i]->K;
+  }
+  // large batches are copied by several threads (one core's memory bandwidth is the limit
+  // otherwise), split into runs of about equal atom counts
+  const std::vector<int64_t> off = atom_offsets(l);
+  const int64_t ao = off[nsys];
+  over_requests(l, off, [&](int i0, int i1) { pack_requests(l, ts, off, i0, i1); });
   cudaStream_t st = l.stream;
   auto h2d = [&](size_t off, size_t bytes) {
     return cudaMemcpyAsync(l.d_in + off, l.h_in + off, bytes, cudaMemcpyHostToDevice, st);
@@ -175,26 +238,6 @@ int launch_lane(tff_server s, Lane &l) {
   TFF_CUDA(cudaMemcpyAsync(l.h_out + l.o_f, l.d_out + l.o_f, 3 * ao * ts, cudaMemcpyDeviceToHost, st));
   TFF_CUDA(cudaEventRecord(l.done_ev, st));
   return TFF_OK;
-}
-
-// Results of a finished lane into the requests' host buffers (worker thread, no lock).
-void unpack_lane(tff_server s, Lane &l) {
-  const double *e = reinterpret_cast<const double *>(l.h_out);
-  int64_t ao = 0;
-  for (size_t i = 0; i < l.reqs.size(); ++i) {
-    ServerReq *r = l.reqs[i];
-    if (r->energy_out) *r->energy_out = e[i];
-    if (r->forces_out) {
-      const int64_t m = 3 * r->n;
-      if (s->ts == 8) {
-        std::memcpy(r->forces_out, l.h_out + l.o_f + 3 * ao * 8, m * 8);
-      } else {
-        const float *f = reinterpret_cast<const float *>(l.h_out + l.o_f) + 3 * ao;
-        for (int64_t k = 0; k < m; ++k) r->forces_out[k] = f[k];
-      }
-    }
-    ao += r->n;
-  }
 }
 
 void worker_loop(tff_server s) {

@@ -103,8 +103,13 @@ __device__ __forceinline__ void pair_min_image(bool ortho, T &dx, T &dy, T &dz, 
   }
 }
 
+// Resident 4-warp blocks per SM the register allocation of the energy kernel must allow
+// (6 blocks = 24 warps: at most 80 registers per thread).
+constexpr int kTileMinBlocks = 6;
+
 template <class T, int MODE = 0>
-__global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32) tile_kernel(TileArgs<T> A) {
+__global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMinBlocks : 1)
+    tile_kernel(TileArgs<T> A) {
   using V = typename V4<T>::type;
   using W2 = typename V2<T>::type;
   constexpr int NW = TileCfg<T, MODE>::NW;
@@ -156,6 +161,14 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32) tile_kernel(TileArg
     const V ci = cl.bc[I], hi_ = cl.bh[I];
     V ui{};
     if constexpr (MODE == 2) ui = A.u[si];
+    // Per-atom shift: every j atom is moved to its image nearest the centre c of cluster I.
+    // If h + rc < L/2 on every axis (h: I's half extent), another image of j would be at
+    // least L - rc away from an i atom while the chosen one is at most h + L/2 away, so every
+    // pair within the cutoff gets its minimum-image displacement and no pair outside the
+    // cutoff can appear inside it.
+    const bool atom_shift = ortho && (hi_.x + (T)A.rc * s_inv[0] < T(0.499)) &&
+                            (hi_.y + (T)A.rc * s_inv[4] < T(0.499)) && (hi_.z + (T)A.rc * s_inv[8] < T(0.499));
+    const T cx = ci.x * s_m[0], cy = ci.y * s_m[4], cz = ci.z * s_m[8];
 
     // stage the tiles and build their cutoff masks (pass 1)
     for (int t = 0; t < ntile; ++t) {
@@ -165,7 +178,7 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32) tile_kernel(TileArg
       // lies within half a box length per axis (orthorhombic boxes)
       bool shifted = false;
       T sx = T(0), sy = T(0), sz = T(0);
-      if (ortho) {
+      if (ortho && !atom_shift) {
         const V cj = cl.bc[J], hj = cl.bh[J];
         const T dcx = ci.x - cj.x, dcy = ci.y - cj.y, dcz = ci.z - cj.z;
         const T nx = floor(dcx + T(0.5)), ny = floor(dcy + T(0.5)), nz = floor(dcz + T(0.5));
@@ -176,7 +189,12 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32) tile_kernel(TileArg
         sz = nz * s_m[8];
       }
       V pj = cl.pos[sj];
-      if (shifted) {
+      if (atom_shift) {
+        pj.x += rint((cx - pj.x) * s_inv[0]) * s_m[0];
+        pj.y += rint((cy - pj.y) * s_inv[4]) * s_m[4];
+        pj.z += rint((cz - pj.z) * s_inv[8]) * s_m[8];
+        shifted = true;
+      } else if (shifted) {
         pj.x += sx;
         pj.y += sy;
         pj.z += sz;
