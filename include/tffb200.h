@@ -84,6 +84,78 @@ int tff_nblist_cell_list(int dtype, int64_t natoms, const void *coords, const vo
                          tff_stream_t stream);
 
 /* ------------------------------------------------------------------------------
+ * Cluster-pair neighbour format
+ * --------------------------------------------------------------------------- */
+
+/* Replaces torch.ops.torchff.build_cluster_pairs (torchff/nblist.py:260-285,
+ * csrc/nblist/nblist_cluster_pairs_cuda.cu:508-657). The format, all on the device:
+ *   sorted_atoms  int32 (nclusters*32)    atom at each slot of the Hilbert-ordered 32-atom
+ *                                         clusters, -1 after the last atom;
+ *   tiles         int32 (2, tiles_cap)    cluster pairs (x, y), x <= y: every diagonal tile
+ *                                         and every tile that holds an excluded pair; row 0 = x,
+ *                                         row 1 = y, -1 padded;
+ *   tile_masks    uint32 (tiles_cap, 32)  row (t, i): bit j set = pair (slot 32x+i, slot 32y+j)
+ *                                         skipped (excluded, padding, or j <= i when x == y);
+ *   entry_cluster int32 (entries_cap)     cluster x of each interacting entry, -1 padded;
+ *   entry_atoms   int32 (entries_cap, 32) atoms of lower clusters that may interact with x
+ *                                         (within the cutoff of x's bounding box), -1 padded.
+ * Every atom pair within the cutoff and not excluded lies in exactly one tile or entry.
+ * Exclusions: symmetric CSR (as for the neighbour lists), NULL = none.
+ * counts (device int64 (3)) receives the numbers of tiles and entries NEEDED and a status
+ * word (bit 0: a cluster has excluded partners in more than 64 clusters; bit 1: a cluster's
+ * neighbour list overflowed max_cluster_neighbors); tiles / entries beyond the capacities
+ * are not written. The outputs are filled with -1 first. nclusters = ceil(natoms / 32). */
+size_t tff_cluster_pairs_workspace_bytes(int dtype, int64_t natoms, int max_cluster_neighbors);
+int tff_cluster_pairs_build(int dtype, int64_t natoms, const void *coords, const void *box,
+                            double cutoff, const int64_t *excl_row_ptr, const int64_t *excl_col,
+                            int32_t *sorted_atoms, int32_t *tiles, uint32_t *tile_masks,
+                            int64_t tiles_cap, int32_t *entry_cluster, int32_t *entry_atoms,
+                            int64_t entries_cap, int64_t *counts, int max_cluster_neighbors,
+                            void *workspace, size_t workspace_bytes, tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.decode_cluster_pairs (torchff/nblist.py:288-311,
+ * csrc/nblist/nblist_cluster_pairs_cuda.cu:364-505, 659-716): every pair of the format within
+ * the cutoff as int32 (larger, smaller) rows of `pairs` (max_npairs, 2), -1 filled first;
+ * *npairs (device int32) = pairs FOUND (may exceed max_npairs). FP32 distances within 1e-5
+ * relative of the cutoff are re-tested in FP64, so the pair set equals the FP64 one. */
+int tff_cluster_pairs_decode(int dtype, int64_t natoms, const void *coords, const void *box,
+                             double cutoff, const int32_t *sorted_atoms, int64_t nslots,
+                             const int32_t *tiles, int64_t ntiles, const uint32_t *tile_masks,
+                             const int32_t *entry_cluster, const int32_t *entry_atoms,
+                             int64_t nentries, int32_t *pairs, int64_t max_npairs, int32_t *npairs,
+                             tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.compute_nonbonded_energy_from_cluster_pairs (schema left
+ * commented out at csrc/nonbonded/nonbonded_interface.cpp:7; kernel
+ * csrc/nonbonded/nonbonded_cluster_pairs_cuda.cu): shifted (do_shift) or plain Coulomb + LJ
+ * (Lorentz-Berthelot from per-atom sigma, epsilon) over the format, with the same pair math
+ * as tff_nonbonded_atom_pairs. Outputs (each nullable): energy (1), its Coulomb part
+ * energy_coulomb (1), dE/dx (N,3), dE/dsigma, dE/depsilon (0 where epsilon_i = 0), dE/dq. */
+size_t tff_nonbonded_cluster_pairs_workspace_bytes(int dtype, int64_t natoms);
+int tff_nonbonded_cluster_pairs(int dtype, int64_t natoms, const void *coords, const void *box,
+                                const void *sigma, const void *epsilon, const void *charges,
+                                double coul_constant, double cutoff, int do_shift,
+                                const int32_t *sorted_atoms, int64_t nslots, const int32_t *tiles,
+                                int64_t ntiles, const uint32_t *tile_masks,
+                                const int32_t *entry_cluster, const int32_t *entry_atoms,
+                                int64_t nentries, void *energy, void *energy_coulomb,
+                                void *grad_coords, void *grad_sigma, void *grad_epsilon,
+                                void *grad_charges, void *workspace, size_t workspace_bytes,
+                                tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.compute_nonbonded_forces_from_cluster_pairs (schema left
+ * commented out at csrc/nonbonded/nonbonded_interface.cpp:8): ADDS the shifted Coulomb + LJ
+ * forces -dE/dx into `forces` (N,3). Workspace as tff_nonbonded_cluster_pairs. */
+int tff_nonbonded_forces_cluster_pairs(int dtype, int64_t natoms, const void *coords,
+                                       const void *box, const void *sigma, const void *epsilon,
+                                       const void *charges, double coul_constant, double cutoff,
+                                       const int32_t *sorted_atoms, int64_t nslots,
+                                       const int32_t *tiles, int64_t ntiles,
+                                       const uint32_t *tile_masks, const int32_t *entry_cluster,
+                                       const int32_t *entry_atoms, int64_t nentries, void *forces,
+                                       void *workspace, size_t workspace_bytes, tff_stream_t stream);
+
+/* ------------------------------------------------------------------------------
  * Pair terms over an explicit pair list
  * --------------------------------------------------------------------------- */
 

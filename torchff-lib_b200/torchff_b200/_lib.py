@@ -64,6 +64,15 @@ _SIGS = {
     "tff_nblist_nsquared": (i32, [i32, i64, vp, vp, f64, vp, vp, i32, vp, i64, vp, vp]),
     "tff_nblist_cell_list_workspace_bytes": (sz, [i32, i64, i32]),
     "tff_nblist_cell_list": (i32, [i32, i64, vp, vp, f64, vp, vp, i32, vp, i64, vp, i32, vp, sz, vp]),
+    "tff_cluster_pairs_workspace_bytes": (sz, [i32, i64, i32]),
+    "tff_cluster_pairs_build": (i32, [i32, i64, vp, vp, f64, vp, vp, vp, vp, vp, i64, vp, vp, i64, vp, i32, vp, sz,
+                                      vp]),
+    "tff_cluster_pairs_decode": (i32, [i32, i64, vp, vp, f64, vp, i64, vp, i64, vp, vp, vp, i64, vp, i64, vp, vp]),
+    "tff_nonbonded_cluster_pairs_workspace_bytes": (sz, [i32, i64]),
+    "tff_nonbonded_cluster_pairs": (i32, [i32, i64, vp, vp, vp, vp, vp, f64, f64, i32, vp, i64, vp, i64, vp, vp, vp,
+                                          i64, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "tff_nonbonded_forces_cluster_pairs": (i32, [i32, i64, vp, vp, vp, vp, vp, f64, f64, vp, i64, vp, i64, vp, vp,
+                                                 vp, i64, vp, vp, sz, vp]),
     "tff_pairs_workspace_bytes": (sz, [i32, i64, i64]),
     "tff_nonbonded_atom_pairs": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, f64, f64, i32, vp, vp, vp, vp, vp,
                                        vp, sz, vp]),

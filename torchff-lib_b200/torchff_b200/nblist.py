@@ -2,7 +2,7 @@
 
 ``NeighborList`` keeps the reference constructor and ``forward`` signature. Both
 algorithms run the sm_100a kernels of libtffb200: ``"nsquared"`` is a shared-memory
-tiled all-pairs test, ``"cell_list"`` bins atoms on a Morton-ordered cell grid, groups
+tiled all-pairs test, ``"cell_list"`` bins atoms on a Hilbert-ordered cell grid, groups
 them in 32-atom clusters and tests cluster pairs with 32x32 warp tiles.
 ``use_customized_ops`` is accepted for signature compatibility; there is no second
 implementation behind it.
@@ -121,3 +121,51 @@ def build_neighbor_list_cell_list(coords: torch.Tensor, box: torch.Tensor, cutof
     pairs, npairs = torch.ops.torchff.build_neighbor_list_cell_list(
         coords, box, cutoff, max_npairs, excl_row_ptr, excl_col_indices, include_self)
     return _trim(pairs, npairs, padding)
+
+
+def build_cluster_pairs(coords: torch.Tensor, box: torch.Tensor, cutoff: float,
+                        exclusions: Optional[torch.Tensor] = None, cell_size: float = 0.4,
+                        max_num_interacting_clusters: int = -1):
+    """Cluster-pair neighbour format (torchff/nblist.py:260-285 signature).
+
+    Returns ``(sorted_atom_indices, cluster_exclusions, bitmask_exclusions,
+    interacting_clusters, interacting_atoms)``:
+
+    - ``sorted_atom_indices`` int32 (nclusters*32,): atom at each slot of the Hilbert-ordered
+      32-atom clusters, -1 after the last atom;
+    - ``cluster_exclusions`` int32 (2, T): cluster pairs (x, y), x <= y, whose 32x32 tile holds
+      an excluded pair, and every diagonal tile;
+    - ``bitmask_exclusions`` uint32 (T, 32): bit j of row (t, i) set = pair (slot 32x+i,
+      slot 32y+j) skipped (excluded, padding, or j <= i when x == y);
+    - ``interacting_clusters`` int32 (M,), ``interacting_atoms`` int32 (M, 32): atoms of lower
+      clusters within the cutoff of cluster x's bounding box, -1 padded.
+
+    Every pair within the cutoff that is not excluded lies in exactly one tile or entry.
+    ``exclusions`` is a (2, E) tensor of excluded atom pairs (either order). With
+    ``max_num_interacting_clusters`` > 0 the entry arrays have that many rows (-1 padded)
+    and a build that needs more raises; -1 sizes them exactly. ``cell_size`` is accepted
+    for signature compatibility: the cell grid is chosen from the atom count.
+    """
+    return torch.ops.torchff.build_cluster_pairs(coords, box, cutoff, exclusions, cell_size,
+                                                 max_num_interacting_clusters)
+
+
+def decode_cluster_pairs(coords: torch.Tensor, box: torch.Tensor, sorted_atom_indices, cluster_exclusions,
+                         bitmask_exclusions, interacting_clusters, interacting_atoms, cutoff: float,
+                         max_npairs: int = -1, padding: bool = False) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Atom pairs of a cluster-pair format within the cutoff (torchff/nblist.py:288-311
+    signature): int32 (P, 2) rows (larger, smaller) and npairs int32 (1,). ``max_npairs`` = -1
+    sizes the output exactly; with ``padding`` the full (max_npairs, 2) buffer is returned,
+    -1 after the found pairs."""
+    return torch.ops.torchff.decode_cluster_pairs(coords, box, sorted_atom_indices, cluster_exclusions,
+                                                  bitmask_exclusions, interacting_clusters, interacting_atoms,
+                                                  cutoff, max_npairs, padding)
+
+
+def build_neighbor_list_cluster_pairs(coords: torch.Tensor, box: torch.Tensor, cutoff: float,
+                                      exclusions: Optional[torch.Tensor], cell_size: float = 0.45,
+                                      max_num_interacting_clusters: int = -1, max_npairs: int = -1,
+                                      padding: bool = False):
+    """Pair list through the cluster-pair format (torchff/nblist.py:314-337)."""
+    nblist = build_cluster_pairs(coords, box, cutoff, exclusions, cell_size, max_num_interacting_clusters)
+    return decode_cluster_pairs(coords, box, *nblist, cutoff, max_npairs, padding)
