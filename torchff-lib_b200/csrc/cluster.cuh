@@ -231,13 +231,20 @@ __device__ void write_box_info(const T *box, double *info) {
   }
 }
 
+// Box facts of one system; the grid also clears `nz` 8-byte words at `z` and `nz2` at `z2`.
 template <class T>
-__global__ void box_info_kernel(const T *box, double *info) {
+__global__ void box_info_kernel(const T *box, double *info, unsigned long long *z = nullptr, int64_t nz = 0,
+                                unsigned long long *z2 = nullptr, int64_t nz2 = 0) {
+  pdl_enter();
   if (threadIdx.x == 0 && blockIdx.x == 0) write_box_info(box, info);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nz; k += stride) z[k] = 0ull;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nz2; k += stride) z2[k] = 0ull;
 }
 
 template <class T>
 __global__ void cell_keys_kernel(const T *x, int64_t n, ClusterData<T> d) {
+  pdl_enter();
   const double *inv = d.boxinfo + 9;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -263,6 +270,7 @@ __global__ void cell_keys_kernel(const T *x, int64_t n, ClusterData<T> d) {
 // threads; thread t owns a contiguous segment, so the work is two sweeps of the segment
 // plus one block-wide scan of the segment sums.
 static __global__ void scan_keys_kernel(unsigned *hist, int64_t nkeys) {
+  pdl_enter();
   __shared__ unsigned s_warp[32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t per = (nkeys + blockDim.x - 1) / blockDim.x;
@@ -299,6 +307,7 @@ static __global__ void scan_keys_kernel(unsigned *hist, int64_t nkeys) {
 
 template <class T>
 __global__ void scatter_atoms_kernel(int64_t n, ClusterData<T> d) {
+  pdl_enter();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     unsigned key = d.keys[i];
@@ -312,6 +321,7 @@ __global__ void scatter_atoms_kernel(int64_t n, ClusterData<T> d) {
 // then the sorted SoA is written. q may be NULL (charge slot = 0).
 template <class T>
 __global__ void sort_buckets_kernel(const T *x, const T *q, int64_t nkeys, ClusterData<T> d) {
+  pdl_enter();
   const double *m = d.boxinfo;
   const double *inv = d.boxinfo + 9;
   const int lane = threadIdx.x & 31;
@@ -504,6 +514,7 @@ __global__ void __launch_bounds__(kBatchSortThreads) batch_sort_kernel(const T *
 // image of it) and widens it by 1e-5 to cover the rounding of centres to T.
 template <class T>
 __global__ void __launch_bounds__(kWarp * kSuper) cluster_bounds_kernel(ClusterData<T> d) {
+  pdl_enter();
   __shared__ double s_box[kSuper][6];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int64_t S = blockIdx.x; S < d.nsuper; S += gridDim.x) {
@@ -612,6 +623,7 @@ __device__ __forceinline__ bool clusters_may_interact(const typename V4<T>::type
 
 template <class T>
 __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) {
+  pdl_enter();
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t I = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); I < d.nclusters; I += nw) {
@@ -703,33 +715,30 @@ __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) 
   if (threadIdx.x == blockDim.x - 1) d.itemoff[n] = run;
 }
 
-// Host driver for steps 1-6 on `stream`.
+// Host driver for steps 1-6 on `stream`. `zero` (`zero_bytes`, a multiple of 8) is cleared
+// on the way. With `pdl` every kernel after the first is a programmatic dependent launch.
 template <class T>
 int build_clusters(const ClusterLayout &L, const ClusterData<T> &d, void *ws, const T *x, const T *q,
-                   const T *box, double rc, int half, cudaStream_t s) {
-  char *b = static_cast<char *>(ws);
-  TFF_CUDA(cudaMemsetAsync(b + L.zero_off, 0, L.zero_bytes, s));
-  box_info_kernel<T><<<1, 32, 0, s>>>(box, d.boxinfo);
-  TFF_LAUNCHED();
-  if (L.natoms == 0) return TFF_OK;
+                   const T *box, double rc, int half, cudaStream_t s, void *zero = nullptr, size_t zero_bytes = 0,
+                   bool pdl = false) {
   const int sms = sm_count();
+  const int64_t nz = (int64_t)(L.zero_bytes / 8);
+  const int nb_zero = (int)std::max<int64_t>(1, std::min<int64_t>((nz + 1023) / 1024, sms));
+  int st = launch_k(false, box_info_kernel<T>, nb_zero, 256, 0, s, box, d.boxinfo,
+                    reinterpret_cast<unsigned long long *>(static_cast<char *>(ws) + L.zero_off), nz,
+                    static_cast<unsigned long long *>(zero), (int64_t)(zero_bytes / 8));
+  if (st != TFF_OK) return st;
+  if (L.natoms == 0) return TFF_OK;
   const int nb_atoms = (int)std::max<int64_t>(1, std::min<int64_t>((L.natoms + 255) / 256, sms * 8));
-  cell_keys_kernel<T><<<nb_atoms, 256, 0, s>>>(x, L.natoms, d);
-  TFF_LAUNCHED();
-  scan_keys_kernel<<<1, 1024, 0, s>>>(d.hist, L.nkeys);
-  TFF_LAUNCHED();
-  scatter_atoms_kernel<T><<<nb_atoms, 256, 0, s>>>(L.natoms, d);
-  TFF_LAUNCHED();
+  if ((st = launch_k(pdl, cell_keys_kernel<T>, nb_atoms, 256, 0, s, x, L.natoms, d)) != TFF_OK) return st;
+  if ((st = launch_k(pdl, scan_keys_kernel, 1, 1024, 0, s, d.hist, L.nkeys)) != TFF_OK) return st;
+  if ((st = launch_k(pdl, scatter_atoms_kernel<T>, nb_atoms, 256, 0, s, L.natoms, d)) != TFF_OK) return st;
   const int nb_keys = (int)std::max<int64_t>(1, std::min<int64_t>((L.nkeys + 3) / 4, sms * 32));
-  sort_buckets_kernel<T><<<nb_keys, 128, 0, s>>>(x, q, L.nkeys, d);
-  TFF_LAUNCHED();
+  if ((st = launch_k(pdl, sort_buckets_kernel<T>, nb_keys, 128, 0, s, x, q, L.nkeys, d)) != TFF_OK) return st;
   const int nb_cl = (int)std::max<int64_t>(1, std::min<int64_t>((L.nclusters + 3) / 4, sms * 16));
   const int nb_super = (int)std::max<int64_t>(1, std::min<int64_t>(L.nsuper, sms * 2));
-  cluster_bounds_kernel<T><<<nb_super, kWarp * kSuper, 0, s>>>(d);
-  TFF_LAUNCHED();
-  cluster_neighbors_kernel<T><<<nb_cl, 128, 0, s>>>(d, rc, half);
-  TFF_LAUNCHED();
-  return TFF_OK;
+  if ((st = launch_k(pdl, cluster_bounds_kernel<T>, nb_super, kWarp * kSuper, 0, s, d)) != TFF_OK) return st;
+  return launch_k(pdl, cluster_neighbors_kernel<T>, nb_cl, 128, 0, s, d, rc, half);
 }
 
 }  // namespace tff

@@ -73,8 +73,7 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
   int st = mark(0, s);
   if (st != TFF_OK) return st;
   const int sms = sm_count();
-  S *energies = reinterpret_cast<S *>(sys->scratch);  // real-space energy accumulators
-  TFF_CUDA(cudaMemsetAsync(sys->scratch, 0, 8 * sizeof(double), s));
+  S *energies = reinterpret_cast<S *>(sys->scratch);  // real-space energy accumulators, zeroed by the build
 
   // --- PME on the side stream: needs only the caller's coordinates and the charges
   const bool use_pme = sys->pme && n > 0;
@@ -105,19 +104,23 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
 
   // --- real space on the caller stream
   ClusterData<T> cd = cluster_data<T>(sys->cl, sys->cl_ws);
+  // the real-space chain (cluster build, sorted parameters, tile kernel) is one run of
+  // programmatic dependent launches unless stage events sit between its kernels
+  const bool pdl = ev == nullptr;
   st = build_clusters<T>(sys->cl, cd, sys->cl_ws, x, static_cast<const T *>(sys->q), box, sys->desc.cutoff,
-                         /*half=*/0, s);
+                         /*half=*/0, s, sys->scratch, 8 * sizeof(double), pdl);
   if (st != TFF_OK) return st;
   if ((st = mark(1, s)) != TFF_OK) return st;
   S *gx = static_cast<S *>(sys->acc);
   S *gq = gx + 3 * sys->cl.npad;
-  TFF_CUDA(cudaMemsetAsync(sys->acc, 0, (size_t)sys->cl.npad * 4 * 8, s));
   auto *lj = static_cast<typename V2<T>::type *>(sys->lj);
   if (n > 0) {
+    // sorted parameters; also zeroes the accumulators
     const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((sys->cl.npad + 255) / 256, sms * 8));
-    sorted_params_kernel<T><<<nb, 256, 0, s>>>(cd, static_cast<const T *>(sys->sigma),
-                                               static_cast<const T *>(sys->eps), sys->excl, lj, sys->exslot);
-    TFF_LAUNCHED();
+    st = launch_k(pdl, sorted_params_kernel<T>, nb, 256, 0, s, cd, static_cast<const T *>(sys->sigma),
+                  static_cast<const T *>(sys->eps), static_cast<const int *>(sys->excl), lj, sys->exslot,
+                  static_cast<const T *>(nullptr), static_cast<typename V4<T>::type *>(nullptr), gx, gq);
+    if (st != TFF_OK) return st;
     TileArgs<T> A;
     A.cl = cd;
     A.lj = lj;
@@ -133,8 +136,7 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
     const int64_t max_items = sys->cl.nclusters * ((sys->cl.cap + kItemTiles - 1) / kItemTiles);
     constexpr int NW = TileCfg<T>::NW;
     const int nbt = (int)std::max<int64_t>(1, std::min<int64_t>((max_items + NW - 1) / NW, (int64_t)sms * 48 / NW));
-    tile_kernel<T><<<nbt, NW * kWarp, 0, s>>>(A);
-    TFF_LAUNCHED();
+    if ((st = launch_k(pdl, tile_kernel<T, 0>, nbt, NW * kWarp, 0, s, A)) != TFF_OK) return st;
   }
   if ((st = mark(2, s)) != TFF_OK) return st;
   if (use_pme) TFF_CUDA(cudaStreamWaitEvent(s, sys->join_ev, 0));

@@ -34,6 +34,36 @@ int sm_count();
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;
 
+// ---------------------------------------------------------------------------------
+// programmatic dependent launch (PTX griddepcontrol, sm_90+)
+// ---------------------------------------------------------------------------------
+// A kernel of a launch chain calls pdl_enter() before anything else: it waits until the
+// grid before it in the stream has completed and its writes are visible (a no-op when the
+// kernel was launched normally), then lets the next grid of the chain begin launching, so
+// that the next kernel's launch overlaps this kernel's run instead of following its end.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launches `kernel` on `s`; with `pdl` as a programmatic dependent of the previous kernel in
+// the stream (the kernel must begin with pdl_enter()).
+template <class... P, class... A>
+int launch_k(bool pdl, void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  TFF_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<P>(args)...));
+  return TFF_OK;
+}
+
 // Workspace carving: 256-byte aligned sub-buffers out of one caller-provided block.
 struct Carver {
   char *base;

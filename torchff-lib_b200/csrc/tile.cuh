@@ -73,11 +73,20 @@ struct TileArgs {
 // from the first atom of the atom's own system (batch mode), i.e. global for one system.
 // With `dir` (caller order (N,3)) also the direction of a second-derivative pass in
 // sorted order.
+// With `gx` / `gq` also zeroes the tile kernel's accumulators of each slot (3 + 1 values).
 template <class T>
 __global__ void sorted_params_kernel(ClusterData<T> cl, const T *sigma, const T *eps, const int *excl,
                                      typename V2<T>::type *lj, int *exslot, const T *dir = nullptr,
-                                     typename V4<T>::type *dir_sorted = nullptr) {
+                                     typename V4<T>::type *dir_sorted = nullptr, typename Acc<T>::S *gx = nullptr,
+                                     typename Acc<T>::S *gq = nullptr) {
+  pdl_enter();
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < cl.npad; s += (int64_t)gridDim.x * blockDim.x) {
+    if (gx) {
+      gx[3 * s] = 0;
+      gx[3 * s + 1] = 0;
+      gx[3 * s + 2] = 0;
+      gq[s] = 0;
+    }
     const int a = cl.sidx[s];
     if (dir)
       dir_sorted[s] = a >= 0 ? make_v4(dir[3 * (int64_t)a], dir[3 * (int64_t)a + 1], dir[3 * (int64_t)a + 2], T(0))
@@ -110,6 +119,7 @@ constexpr int kTileMinBlocks = 6;
 template <class T, int MODE = 0>
 __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMinBlocks : 1)
     tile_kernel(TileArgs<T> A) {
+  pdl_enter();
   using V = typename V4<T>::type;
   using W2 = typename V2<T>::type;
   constexpr int NW = TileCfg<T, MODE>::NW;
@@ -516,6 +526,7 @@ __global__ void finalize_kernel(ClusterData<T> cl, const typename Acc<T>::S *gx,
                                 const T *pme_grad, const T *pme_phi, T *forces, double *forces64, T *grad_q,
                                 const typename Acc<T>::S *e_tile_acc, const double *e_pme, double kc,
                                 double *energy, double *terms, int nsys) {
+  pdl_enter();
   for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < cl.natoms;
        a += (int64_t)gridDim.x * blockDim.x) {
     const int64_t s = cl.inv[a];
