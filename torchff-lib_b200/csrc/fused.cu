@@ -141,10 +141,11 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
   if ((st = mark(2, s)) != TFF_OK) return st;
   if (use_pme) TFF_CUDA(cudaStreamWaitEvent(s, sys->join_ev, 0));
   const int nbf = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sms * 8));
-  finalize_kernel<T><<<nbf, 256, 0, s>>>(cd, gx, gq, use_pme ? static_cast<const T *>(sys->pme_grad) : nullptr,
-                                         use_pme ? static_cast<const T *>(sys->pme_phi) : nullptr, forces, forces64,
-                                         grad_q, energies, e_pme, sys->desc.coul_constant, energy, terms, 1);
-  TFF_LAUNCHED();
+  st = launch_k(pdl, finalize_kernel<T>, nbf, 256, 0, s, cd, static_cast<const S *>(gx), static_cast<const S *>(gq),
+                use_pme ? static_cast<const T *>(sys->pme_grad) : static_cast<const T *>(nullptr),
+                use_pme ? static_cast<const T *>(sys->pme_phi) : static_cast<const T *>(nullptr), forces, forces64,
+                grad_q, static_cast<const S *>(energies), e_pme, sys->desc.coul_constant, energy, terms, 1);
+  if (st != TFF_OK) return st;
   return mark(5, s);
 }
 

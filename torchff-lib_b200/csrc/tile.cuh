@@ -127,9 +127,9 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
   __shared__ V s_u[NW][kItemTiles][MODE == 2 ? kWarp : 1];  // MODE 2: direction of the j atoms
   __shared__ W2 s_lj[NW][kItemTiles][kWarp];
   // negated j positions, structure of arrays, for the packed FP32 distance pass
-  __shared__ __align__(8) float s_nx[NW][kItemTiles][sizeof(T) == 4 ? kWarp : 2];
-  __shared__ __align__(8) float s_ny[NW][kItemTiles][sizeof(T) == 4 ? kWarp : 2];
-  __shared__ __align__(8) float s_nz[NW][kItemTiles][sizeof(T) == 4 ? kWarp : 2];
+  __shared__ __align__(16) float s_nx[NW][kItemTiles][sizeof(T) == 4 ? kWarp : 4];
+  __shared__ __align__(16) float s_ny[NW][kItemTiles][sizeof(T) == 4 ? kWarp : 4];
+  __shared__ __align__(16) float s_nz[NW][kItemTiles][sizeof(T) == 4 ? kWarp : 4];
   __shared__ unsigned s_mask[NW][kItemTiles][kWarp];   // in-cutoff, not excluded
   __shared__ unsigned s_xmask[NW][kItemTiles][kWarp];  // in-cutoff, excluded
   __shared__ int s_mi[NW][kItemTiles];                 // 1: tile needs the per-pair minimum image
@@ -140,6 +140,7 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
   int cur_sys = -1;
   bool ortho = false;
   const T rc2 = (T)(A.rc * A.rc);
+  const float rc2_up = nextafterf((float)(A.rc * A.rc), INFINITY);  // FP32 pass 1: r2 <= rc2 <=> r2 < rc2_up
   const T alpha = (T)A.alpha;
   const T kc = (T)A.kc;
   const T two_a_rpi = (T)(2.0 * A.alpha / 1.7724538509055160273);
@@ -179,6 +180,12 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
     const bool atom_shift = ortho && (hi_.x + (T)A.rc * s_inv[0] < T(0.499)) &&
                             (hi_.y + (T)A.rc * s_inv[4] < T(0.499)) && (hi_.z + (T)A.rc * s_inv[8] < T(0.499));
     const T cx = ci.x * s_m[0], cy = ci.y * s_m[4], cz = ci.z * s_m[8];
+
+    // excluded partners of atom i as sorted slots (-1: none; -1 >> 5 never equals a cluster)
+    int xs_i[kMaxExcl];
+#pragma unroll
+    for (int x = 0; x < kMaxExcl; ++x) xs_i[x] = A.exslot[si * kMaxExcl + x];
+    bool all_shifted = true;  // warp-uniform: no tile of the item needs the per-pair minimum image
 
     // stage the tiles and build their cutoff masks (pass 1)
     for (int t = 0; t < ntile; ++t) {
@@ -221,22 +228,35 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
       __syncwarp();
       unsigned mask = 0u;
       if (sizeof(T) == 4 && shifted) {
-        // two j atoms per step with paired FP32 instructions (FADD2/FMUL2/FFMA2)
+        // four j atoms per shared load, two per paired FP32 instruction (FADD2/FFMA2). The
+        // FMA chain starts from -rc2' (rc2' = the float just above rc^2), so its result is
+        // negative exactly for the pairs inside the cutoff and the sign bit is the mask bit:
+        // a funnel shift appends it (first atom ends in bit 31; reversed once per tile).
         const float2 px = make_float2((float)pi.x, (float)pi.x), py = make_float2((float)pi.y, (float)pi.y),
                      pz = make_float2((float)pi.z, (float)pi.z);
-        const float rc2f = (float)rc2;
-#pragma unroll 4
-        for (int s = 0; s < kWarp; s += 2) {
-          const float2 nx = *reinterpret_cast<const float2 *>(&s_nx[w][t][s]);
-          const float2 ny = *reinterpret_cast<const float2 *>(&s_ny[w][t][s]);
-          const float2 nz = *reinterpret_cast<const float2 *>(&s_nz[w][t][s]);
-          const float2 dx = __fadd2_rn(px, nx), dy = __fadd2_rn(py, ny), dz = __fadd2_rn(pz, nz);
-          float2 r2 = __fmul2_rn(dx, dx);
-          r2 = __ffma2_rn(dy, dy, r2);
-          r2 = __ffma2_rn(dz, dz, r2);
-          mask |= (r2.x <= rc2f ? 1u : 0u) << s;
-          mask |= (r2.y <= rc2f ? 2u : 0u) << s;
+        const float2 nrc2 = make_float2(-rc2_up, -rc2_up);
+#pragma unroll 2
+        for (int s = 0; s < kWarp; s += 4) {
+          const float4 nx = *reinterpret_cast<const float4 *>(&s_nx[w][t][s]);
+          const float4 ny = *reinterpret_cast<const float4 *>(&s_ny[w][t][s]);
+          const float4 nz = *reinterpret_cast<const float4 *>(&s_nz[w][t][s]);
+          float2 dx = __fadd2_rn(px, make_float2(nx.x, nx.y)), dy = __fadd2_rn(py, make_float2(ny.x, ny.y)),
+                 dz = __fadd2_rn(pz, make_float2(nz.x, nz.y));
+          float2 d2 = __ffma2_rn(dx, dx, nrc2);
+          d2 = __ffma2_rn(dy, dy, d2);
+          d2 = __ffma2_rn(dz, dz, d2);
+          mask = __funnelshift_l(__float_as_uint(d2.x), mask, 1);
+          mask = __funnelshift_l(__float_as_uint(d2.y), mask, 1);
+          dx = __fadd2_rn(px, make_float2(nx.z, nx.w));
+          dy = __fadd2_rn(py, make_float2(ny.z, ny.w));
+          dz = __fadd2_rn(pz, make_float2(nz.z, nz.w));
+          d2 = __ffma2_rn(dx, dx, nrc2);
+          d2 = __ffma2_rn(dy, dy, d2);
+          d2 = __ffma2_rn(dz, dz, d2);
+          mask = __funnelshift_l(__float_as_uint(d2.x), mask, 1);
+          mask = __funnelshift_l(__float_as_uint(d2.y), mask, 1);
         }
+        mask = __brev(mask);
       } else {
 #pragma unroll 8
         for (int s = 0; s < kWarp; ++s) {
@@ -253,14 +273,13 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
       unsigned emask = 0u;
       if (mask) {
 #pragma unroll
-        for (int x = 0; x < kMaxExcl; ++x) {
-          const int xs = A.exslot[si * kMaxExcl + x];
-          if (xs >= 0 && (xs >> 5) == J) emask |= 1u << (xs & 31);
-        }
+        for (int x = 0; x < kMaxExcl; ++x)
+          if ((xs_i[x] >> 5) == J) emask |= 1u << (xs_i[x] & 31);
       }
       s_mask[w][t][lane] = mask & ~emask;
       s_xmask[w][t][lane] = mask & emask;
       if (lane == 0) s_mi[w][t] = !shifted;
+      all_shifted = all_shifted && shifted;
     }
     __syncwarp();
 
@@ -309,8 +328,10 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
           float2 dx = __fadd2_rn(pix, make_float2(-qa.x, -qb.x));
           float2 dy = __fadd2_rn(piy, make_float2(-qa.y, -qb.y));
           float2 dz = __fadd2_rn(piz, make_float2(-qa.z, -qb.z));
-          if (s_mi[w][ta]) pair_min_image(ortho, dx.x, dy.x, dz.x, s_m, s_inv);
-          if (hb && s_mi[w][tb]) pair_min_image(ortho, dx.y, dy.y, dz.y, s_m, s_inv);
+          if (!all_shifted) {
+            if (s_mi[w][ta]) pair_min_image(ortho, dx.x, dy.x, dz.x, s_m, s_inv);
+            if (hb && s_mi[w][tb]) pair_min_image(ortho, dx.y, dy.y, dz.y, s_m, s_inv);
+          }
           float2 r2 = __fmul2_rn(dx, dx);
           r2 = __ffma2_rn(dy, dy, r2);
           r2 = __ffma2_rn(dz, dz, r2);
