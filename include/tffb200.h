@@ -237,6 +237,52 @@ int tff_ewald_real_atom_pairs(int dtype, int64_t natoms, const void *coords, con
                               size_t workspace_bytes, tff_stream_t stream);
 
 /* ------------------------------------------------------------------------------
+ * Bonded terms (flexible water): harmonic bonds and angles
+ * --------------------------------------------------------------------------- */
+
+/* Workspace of every bonded entry point below (nterms = bonds or angles of the call). */
+size_t tff_bonded_workspace_bytes(int dtype, int64_t natoms, int64_t nterms);
+
+/* Replaces torch.ops.torchff.compute_harmonic_bond_energy (csrc/bond/bond_interface.cpp:5,
+ * csrc/bond/harmonic_bond_cuda.cu:78-142; torchff/bond.py:9-43):
+ * E = sum 1/2 k_m (r_m - b0_m)^2, r_m = |x_j - x_i| for bonds (M,2) int64 (no periodic image,
+ * as the reference). Outputs (each nullable): energy (1), dE/dx (N,3), dE/db0 (M,), dE/dk (M,). */
+int tff_harmonic_bond(int dtype, int64_t natoms, const void *coords, int64_t nbonds,
+                      const int64_t *bonds, const void *b0, const void *k, void *energy,
+                      void *grad_coords, void *grad_b0, void *grad_k, void *workspace,
+                      size_t workspace_bytes, tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.compute_harmonic_bond_forces (csrc/bond/bond_interface.cpp:6,
+ * csrc/bond/harmonic_bond_cuda.cu:145-175): ADDS -dE/dx into `forces` (N,3). */
+int tff_harmonic_bond_forces(int dtype, int64_t natoms, const void *coords, int64_t nbonds,
+                             const int64_t *bonds, const void *b0, const void *k, void *forces,
+                             void *workspace, size_t workspace_bytes, tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.compute_harmonic_angle_energy (csrc/angle/angle_interface.cpp:5,
+ * csrc/angle/harmonic_angle_cuda.cu:104-169; torchff/angle.py:78-112): E = sum 1/2 k (theta -
+ * theta0)^2, theta the angle at the central atom j of each (i, j, k) row of angles (M,3) int64.
+ * Outputs (each nullable): energy (1), dE/dx (N,3), dE/dtheta0 (M,), dE/dk (M,). Straight angles
+ * use sin(theta) >= 1e-15 instead of the unbounded derivative. */
+int tff_harmonic_angle(int dtype, int64_t natoms, const void *coords, int64_t nangles,
+                       const int64_t *angles, const void *theta0, const void *k, void *energy,
+                       void *grad_coords, void *grad_theta0, void *grad_k, void *workspace,
+                       size_t workspace_bytes, tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.compute_harmonic_angle_forces (csrc/angle/angle_interface.cpp:6,
+ * csrc/angle/harmonic_angle_cuda.cu:172-204): ADDS -dE/dx into `forces` (N,3). */
+int tff_harmonic_angle_forces(int dtype, int64_t natoms, const void *coords, int64_t nangles,
+                              const int64_t *angles, const void *theta0, const void *k,
+                              void *forces, void *workspace, size_t workspace_bytes,
+                              tff_stream_t stream);
+
+/* Replaces torch.ops.torchff.compute_angles and its backward (csrc/angle/angle_interface.cpp:7,
+ * csrc/angle/angles_cuda.cu:83-160; torchff/angle.py:8-55): theta (M,) of every angle (nullable);
+ * with grad_theta (M,) also dE/dx = sum grad_theta dtheta/dx into grad_coords (N,3). */
+int tff_angles(int dtype, int64_t natoms, const void *coords, int64_t nangles,
+               const int64_t *angles, void *theta, const void *grad_theta, void *grad_coords,
+               void *workspace, size_t workspace_bytes, tff_stream_t stream);
+
+/* ------------------------------------------------------------------------------
  * PME reciprocal space (rank 0, order-6 B-splines, cubic K x K x K grid)
  * --------------------------------------------------------------------------- */
 
@@ -263,7 +309,8 @@ int tff_pme_long_range(tff_pme_plan plan, int64_t natoms, const void *coords, co
 /* ------------------------------------------------------------------------------
  * Fused fixed-charge system: cluster-pair neighbour build + fused real-space
  * LJ / erfc-Coulomb with exclusion correction + PME, energy and forces in one call.
- * This is the evaluation of examples/tip3p/model.py:100-133 (nonbonded terms).
+ * This is the evaluation of examples/tip3p/model.py:100-133 (nonbonded terms, plus the
+ * harmonic bonds and angles of a flexible model through tff_system_set_bonded).
  * --------------------------------------------------------------------------- */
 
 typedef struct tff_system_s *tff_system;
@@ -289,10 +336,21 @@ int tff_system_destroy(tff_system sys);
 /* Overwrites per-atom parameters (device arrays of the system dtype, may be NULL to keep). */
 int tff_system_set_parameters(tff_system sys, const void *charges, const void *sigma,
                               const void *epsilon, tff_stream_t stream);
+/* Adds (or, with nbonds = nangles = 0, removes) the harmonic bonds and angles of a flexible
+ * model (examples/tip3p/model.py:105-106: HarmonicBond + HarmonicAngle, torchff/bond.py,
+ * torchff/angle.py) to the system. HOST arrays: bonds (nbonds, 2) int64, b0, kb (nbonds);
+ * angles (nangles, 3) int64 (central atom in the middle), theta0 (rad), ktheta (nangles).
+ * They are evaluated in every tff_system_eval / _eval_host / _eval_grads (energy and forces;
+ * bond lengths use no periodic image, as the reference); tff_system_hvp then returns
+ * TFF_ERR_INVALID. Synchronises the device; call it outside stream capture. */
+int tff_system_set_bonded(tff_system sys, int64_t nbonds, const int64_t *bonds, const double *b0,
+                          const double *kb, int64_t nangles, const int64_t *angles,
+                          const double *theta0, const double *ktheta);
 /* Evaluates energy and forces with device-resident inputs. coords (N,3), box (3,3) in the
  * system dtype; energy (device double, 1) total in kJ/mol; forces (N,3) system dtype,
- * = -dE/dx; grad_charges (N) optional dE/dq. energy_terms (device double, 4) optional:
- * real-space pairs, exclusion correction, reciprocal, self. */
+ * = -dE/dx; grad_charges (N) optional dE/dq. energy_terms (device double) optional:
+ * real-space pairs, exclusion correction, reciprocal, self (4 values), then bonds and
+ * angles (6 values) when the system has bonded terms. */
 int tff_system_eval(tff_system sys, const void *coords, const void *box, double *energy,
                     void *forces, void *grad_charges, double *energy_terms, tff_stream_t stream);
 /* Same with HOST buffers: copies coords/box in, evaluates, copies energy/forces out and

@@ -19,7 +19,9 @@ It restates, in float64 numpy, the reference's pure-torch path (THGLab/torchff-l
 * rank-0 real-space Ewald Coulomb with the erfc-1 exclusion correction
   (``torchff/multipoles.py:106-127, 244-341``);
 * rank-0 smooth PME reciprocal space with order-6 B-splines
-  (``torchff/pme_ref.py:11-469``, ``torchff/pme.py:67-126``).
+  (``torchff/pme_ref.py:11-469``, ``torchff/pme.py:67-126``);
+* harmonic bonds and angles of flexible water (``torchff/bond.py:34-43``,
+  ``torchff/angle.py:8-34, 103-112``).
 
 Energies and all first derivatives are analytic. The tests pin this module against the
 golden fixtures in ``tests/golden`` which were produced by running the reference's own
@@ -399,6 +401,74 @@ def pme(coords, box, q, alpha, K):
     pot = phi - 2.0 * alpha / math.sqrt(math.pi) * q
     energy = 0.5 * float(np.sum(q * pot))
     return energy, gx, pot, Phi
+
+
+# ---------------------------------------------------------------------------
+# bonded terms (flexible water)
+# ---------------------------------------------------------------------------
+
+
+def harmonic_bond(coords, bonds, b0, k):
+    """E = sum 1/2 k (r - b0)^2 over bonds (i, j), r = |x_j - x_i| with no periodic image.
+
+    Restates ``compute_harmonic_bond_energy_ref`` (``torchff/bond.py:34-43``). Returns E,
+    dE/dx (N,3), dE/db0 (M,), dE/dk (M,).
+    """
+    x = np.asarray(coords, np.float64)
+    b = np.asarray(bonds, np.int64)
+    b0 = np.asarray(b0, np.float64)
+    k = np.asarray(k, np.float64)
+    d = x[b[:, 1]] - x[b[:, 0]]
+    r = np.linalg.norm(d, axis=1)
+    dr = r - b0
+    e = float(np.sum(0.5 * k * dr * dr))
+    g = (k * dr / r)[:, None] * d  # dE/dx_j; dE/dx_i = -g
+    gx = np.zeros_like(x)
+    np.add.at(gx, b[:, 1], g)
+    np.add.at(gx, b[:, 0], -g)
+    return e, gx, -k * dr, 0.5 * dr * dr
+
+
+def angles(coords, triples):
+    """Angle at the central atom j of each (i, j, k), radians (``torchff/angle.py:8-34``)."""
+    x = np.asarray(coords, np.float64)
+    a = np.asarray(triples, np.int64)
+    v1 = x[a[:, 0]] - x[a[:, 1]]
+    v2 = x[a[:, 2]] - x[a[:, 1]]
+    c = np.sum(v1 * v2, 1) / (np.linalg.norm(v1, axis=1) * np.linalg.norm(v2, axis=1))
+    return np.arccos(np.clip(c, -1.0, 1.0))
+
+
+def harmonic_angle(coords, triples, theta0, k):
+    """E = sum 1/2 k (theta - theta0)^2 (``compute_harmonic_angle_energy_ref``,
+    ``torchff/angle.py:103-112``). Returns E, dE/dx, dE/dtheta0, dE/dk.
+
+    With u = v1/|v1|, w = v2/|v2| and c = u.w: dtheta/dv1 = -(w - c u) / (|v1| sin theta),
+    dtheta/dv2 = -(u - c w) / (|v2| sin theta).
+    """
+    x = np.asarray(coords, np.float64)
+    a = np.asarray(triples, np.int64)
+    th0 = np.asarray(theta0, np.float64)
+    k = np.asarray(k, np.float64)
+    v1 = x[a[:, 0]] - x[a[:, 1]]
+    v2 = x[a[:, 2]] - x[a[:, 1]]
+    n1 = np.linalg.norm(v1, axis=1)
+    n2 = np.linalg.norm(v2, axis=1)
+    u = v1 / n1[:, None]
+    w = v2 / n2[:, None]
+    c = np.clip(np.sum(u * w, 1), -1.0, 1.0)
+    th = np.arccos(c)
+    s = np.sqrt(np.maximum(1.0 - c * c, 1e-300))
+    dth = th - th0
+    e = float(np.sum(0.5 * k * dth * dth))
+    f = k * dth
+    g1 = (f / (n1 * s))[:, None] * -(w - c[:, None] * u)
+    g3 = (f / (n2 * s))[:, None] * -(u - c[:, None] * w)
+    gx = np.zeros_like(x)
+    np.add.at(gx, a[:, 0], g1)
+    np.add.at(gx, a[:, 2], g3)
+    np.add.at(gx, a[:, 1], -g1 - g3)
+    return e, gx, -f, 0.5 * dth * dth
 
 
 # ---------------------------------------------------------------------------

@@ -17,14 +17,18 @@ float64 with autograd and stores inputs and outputs as small ``.npz`` files:
 * ``pairs_random.npz``   -- shifted Coulomb (torchff/coulomb.py:22-44) and LJ
                             (torchff/vdw.py:86-111) composed with Lorentz-Berthelot
                             combining, the fused term torchff/nonbonded.py:40-69 intends,
-                            on seeded random atoms with per-atom parameters.
+                            on seeded random atoms with per-atom parameters;
+* ``bonded_water.npz``   -- harmonic bonds and angles (torchff/bond.py HarmonicBond,
+                            torchff/angle.py HarmonicAngle and compute_angles_ref) of 216
+                            flexible waters with distorted geometry and perturbed parameters:
+                            energies, angles and autograd gradients.
 
 The reference's compiled extension modules are replaced by empty stubs (the pure-torch
 path never calls them). ``torchff/pme_ref.py`` switches the default device to CUDA at
 import time, so the default device is reset to CPU afterwards.
 
 Usage (needs a checkout of the reference; not run by the test-suite):
-    python tests/golden/make_golden.py /path/to/torchff-lib
+    python tests/golden/make_golden.py /path/to/torchff-lib [fixture names ...]
 """
 from __future__ import annotations
 
@@ -40,7 +44,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(REPO, "torchff-lib_b200"))
 
-from torchff_b200.water import water_box_216, water_exclusions  # noqa: E402
+from torchff_b200.water import water_bonded_terms, water_box_216, water_exclusions  # noqa: E402
 
 
 def import_reference(ref_root: str):
@@ -55,11 +59,14 @@ def import_reference(ref_root: str):
     from torchff.pme import PME
     from torchff.vdw import Vdw, compute_lennard_jones_energy_ref
     from torchff.coulomb import compute_coulomb_energy_ref
+    from torchff.bond import HarmonicBond
+    from torchff.angle import HarmonicAngle, compute_angles_ref
     torch.set_default_device("cpu")
     torch.set_default_dtype(torch.float64)
     return types.SimpleNamespace(
         NeighborList=NeighborList, MultipolarInteraction=MultipolarInteraction, PME=PME, Vdw=Vdw,
         lj_ref=compute_lennard_jones_energy_ref, coul_ref=compute_coulomb_energy_ref,
+        HarmonicBond=HarmonicBond, HarmonicAngle=HarmonicAngle, angles_ref=compute_angles_ref,
     )
 
 
@@ -237,16 +244,45 @@ def gen_pairs_random(ref) -> dict:
     return out
 
 
+def gen_bonded_water(ref) -> dict:
+    wb = water_box_216(seed=3)
+    bt = water_bonded_terms(wb.n_waters)
+    rng = np.random.default_rng(7)
+    coords_np = wb.coords + rng.normal(0.0, 0.006, wb.coords.shape)
+    b0_np = bt.b0 * (1.0 + rng.uniform(-0.03, 0.03, bt.b0.shape))
+    kb_np = bt.kb * (1.0 + rng.uniform(-0.1, 0.1, bt.kb.shape))
+    th0_np = bt.th0 + rng.uniform(-0.05, 0.05, bt.th0.shape)
+    kth_np = bt.kth * (1.0 + rng.uniform(-0.1, 0.1, bt.kth.shape))
+    x = torch.tensor(coords_np, requires_grad=True)
+    b0 = torch.tensor(b0_np, requires_grad=True)
+    kb = torch.tensor(kb_np, requires_grad=True)
+    e_b = ref.HarmonicBond(use_customized_ops=False)(x, torch.tensor(bt.bonds), b0, kb)
+    gx_b, gb0, gkb = torch.autograd.grad(e_b, (x, b0, kb))
+    th0 = torch.tensor(th0_np, requires_grad=True)
+    kth = torch.tensor(kth_np, requires_grad=True)
+    x2 = torch.tensor(coords_np, requires_grad=True)
+    e_a = ref.HarmonicAngle(use_customized_ops=False)(x2, torch.tensor(bt.angles), th0, kth)
+    gx_a, gth0, gkth = torch.autograd.grad(e_a, (x2, th0, kth))
+    theta = ref.angles_ref(torch.tensor(coords_np), torch.tensor(bt.angles))
+    return {"coords": coords_np, "bonds": bt.bonds, "b0": b0_np, "kb": kb_np, "angles": bt.angles,
+            "th0": th0_np, "kth": kth_np, "bond_energy": np.float64(e_b.item()), "bond_gx": gx_b.numpy(),
+            "bond_gb0": gb0.numpy(), "bond_gk": gkb.numpy(), "angle_energy": np.float64(e_a.item()),
+            "angle_gx": gx_a.numpy(), "angle_gth0": gth0.numpy(), "angle_gk": gkth.numpy(),
+            "theta": theta.numpy()}
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TORCHFF_REFERENCE", "")
     if not ref_root or not os.path.isdir(ref_root):
         raise SystemExit("usage: make_golden.py /path/to/torchff-lib")
     ref = import_reference(ref_root)
-    np.savez_compressed(os.path.join(HERE, "nblist_small.npz"), **gen_nblist_small(ref))
-    np.savez_compressed(os.path.join(HERE, "water216.npz"), **gen_water216(ref))
-    np.savez_compressed(os.path.join(HERE, "pme_random300.npz"), **gen_pme_random300(ref, ref_root))
-    np.savez_compressed(os.path.join(HERE, "pairs_random.npz"), **gen_pairs_random(ref))
-    print("golden fixtures written to", HERE)
+    gens = {"nblist_small": lambda: gen_nblist_small(ref), "water216": lambda: gen_water216(ref),
+            "pme_random300": lambda: gen_pme_random300(ref, ref_root), "pairs_random": lambda: gen_pairs_random(ref),
+            "bonded_water": lambda: gen_bonded_water(ref)}
+    names = sys.argv[2:] or list(gens)
+    for name in names:
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **gens[name]())
+    print("golden fixtures written to", HERE, names)
 
 
 if __name__ == "__main__":

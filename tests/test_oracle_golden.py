@@ -91,3 +91,16 @@ def test_bspline_partition_of_unity():
     ders = np.stack([O.bspline6(w + k)[1] for k in range(6)], 0)
     assert np.allclose(vals.sum(0), 1.0, atol=1e-14)
     assert np.allclose(ders.sum(0), 0.0, atol=1e-13)
+
+
+def test_bonded_water():
+    """Harmonic bonds / angles and the angle values against the reference's pure-torch
+    HarmonicBond, HarmonicAngle and compute_angles_ref (flexible 216-water box)."""
+    g = np.load(os.path.join(GOLDEN, "bonded_water.npz"))
+    e, gx, gb0, gk = O.harmonic_bond(g["coords"], g["bonds"], g["b0"], g["kb"])
+    assert abs(e - float(g["bond_energy"])) <= 1e-13 * abs(float(g["bond_energy"]))
+    assert _rel(gx, g["bond_gx"]) < 1e-12 and _rel(gb0, g["bond_gb0"]) < 1e-12 and _rel(gk, g["bond_gk"]) < 1e-12
+    e, gx, gt, gk = O.harmonic_angle(g["coords"], g["angles"], g["th0"], g["kth"])
+    assert abs(e - float(g["angle_energy"])) <= 1e-13 * abs(float(g["angle_energy"]))
+    assert _rel(gx, g["angle_gx"]) < 1e-12 and _rel(gt, g["angle_gth0"]) < 1e-12 and _rel(gk, g["angle_gk"]) < 1e-12
+    assert np.max(np.abs(O.angles(g["coords"], g["angles"]) - g["theta"])) < 1e-14

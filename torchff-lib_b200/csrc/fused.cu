@@ -47,6 +47,12 @@ struct tff_system_s {
   double *dev_e = nullptr;
   cudaGraphExec_t host_graph = nullptr;  // device part of tff_system_eval_host, captured once
   cudaStream_t capture_stream = nullptr;
+  // bonded terms (flexible water), set by tff_system_set_bonded
+  int64_t nbonds = 0, nangles = 0;
+  int64_t *bonds = nullptr, *angles = nullptr;  // (M,2), (M,3)
+  void *bpar = nullptr;                         // b0, kb (nbonds each), th0, kth (nangles each), system dtype
+  void *bacc = nullptr;                         // caller-order dE/dx (3N) + bond, angle energies
+  bool has_bonded() const { return nbonds + nangles > 0; }
 };
 
 namespace tff {
@@ -61,6 +67,22 @@ int record_event(cudaEvent_t e, cudaStream_t s) {
     TFF_CUDA(cudaEventRecordWithFlags(e, s, cudaEventRecordExternal));
   else
     TFF_CUDA(cudaEventRecord(e, s));
+  return TFF_OK;
+}
+
+// Bonds and angles of the system into sys->bacc on stream s (zeroed first).
+template <class T>
+int launch_bonded(tff_system sys, const T *x, cudaStream_t s) {
+  const int64_t n = sys->desc.natoms;
+  TFF_CUDA(cudaMemsetAsync(sys->bacc, 0, (3 * n + 2) * 8, s));
+  const T *p = static_cast<const T *>(sys->bpar);
+  const int64_t nt = sys->nbonds + sys->nangles;
+  const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((nt + kBondBlock - 1) / kBondBlock, (int64_t)sm_count() * 4));
+  system_bonded_kernel<T><<<nb, kBondBlock, 0, s>>>(x, n, sys->bonds, sys->nbonds, p, p + sys->nbonds, sys->angles,
+                                                    sys->nangles, p + 2 * sys->nbonds,
+                                                    p + 2 * sys->nbonds + sys->nangles,
+                                                    static_cast<typename Acc<T>::S *>(sys->bacc));
+  TFF_LAUNCHED();
   return TFF_OK;
 }
 
@@ -89,6 +111,8 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
     char *pw = static_cast<char *>(sys->pme_ws);
     PlainAtoms<T> atoms{x, static_cast<const T *>(sys->q), n};
     T *phi_grid = nullptr;
+    // bonded terms ride on the PME stream (a few microseconds, off the real-space chain)
+    if (sys->has_bonded() && (st = launch_bonded<T>(sys, x, ps)) != TFF_OK) return st;
     st = pme_grid_phase<T>(sys->pme->impl, sys->pl, pw, atoms, n, box, sys->desc.ewald_alpha, xm, ym, zm, ps,
                            &phi_grid);
     if (st != TFF_OK) return st;
@@ -101,6 +125,8 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
     TFF_CUDA(cudaEventRecord(sys->join_ev, ps));
     e_pme = reinterpret_cast<const double *>(pw + sys->pl.energies);
   }
+
+  if (!use_pme && sys->has_bonded() && n > 0 && (st = launch_bonded<T>(sys, x, s)) != TFF_OK) return st;
 
   // --- real space on the caller stream
   ClusterData<T> cd = cluster_data<T>(sys->cl, sys->cl_ws);
@@ -144,7 +170,8 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
   st = launch_k(pdl, finalize_kernel<T>, nbf, 256, 0, s, cd, static_cast<const S *>(gx), static_cast<const S *>(gq),
                 use_pme ? static_cast<const T *>(sys->pme_grad) : static_cast<const T *>(nullptr),
                 use_pme ? static_cast<const T *>(sys->pme_phi) : static_cast<const T *>(nullptr), forces, forces64,
-                grad_q, static_cast<const S *>(energies), e_pme, sys->desc.coul_constant, energy, terms, 1);
+                grad_q, static_cast<const S *>(energies), e_pme, sys->desc.coul_constant, energy, terms, 1,
+                sys->has_bonded() && n > 0 ? static_cast<const S *>(sys->bacc) : static_cast<const S *>(nullptr));
   if (st != TFF_OK) return st;
   return mark(5, s);
 }
@@ -153,11 +180,12 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
 // dE/dq, dE/dsigma, dE/deps, energy) and MODE 2 (the same slots hold the derivatives of
 // dir . dE/dx). pme_vec / pme_scal are the PME parts (already scaled by kc in MODE 2).
 // dE/deps_i = (dE/da_i) / (2 a_i) with a = sqrt(eps), and 0 where eps_i = 0.
+// With `bonded` (MODE 1) the bonded dE/dx and energies are added as in finalize_kernel.
 template <class T, int MODE>
 __global__ void finalize_grads_kernel(ClusterData<T> cl, const typename Acc<T>::S *acc, const T *pme_vec,
                                       const T *pme_scal, const T *eps, double kc, T *out_x, T *out_q, T *out_s,
                                       T *out_e, const typename Acc<T>::S *e_tile, const double *e_pme,
-                                      double *energy) {
+                                      double *energy, const typename Acc<T>::S *bonded) {
   using S = typename Acc<T>::S;
   const int64_t np = cl.npad;
   const S *gx = acc, *gq = acc + 3 * np, *gs = acc + 4 * np, *ga = acc + 5 * np;
@@ -166,7 +194,9 @@ __global__ void finalize_grads_kernel(ClusterData<T> cl, const typename Acc<T>::
     const int64_t s = cl.inv[a];
     double x[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) x[c] = Acc<T>::get(&gx[3 * s + c]) + (pme_vec ? ps * (double)pme_vec[3 * a + c] : 0.0);
+    for (int c = 0; c < 3; ++c)
+      x[c] = Acc<T>::get(&gx[3 * s + c]) + (pme_vec ? ps * (double)pme_vec[3 * a + c] : 0.0) +
+             (bonded ? Acc<T>::get(&bonded[3 * a + c]) : 0.0);
     if (out_x)
 #pragma unroll
       for (int c = 0; c < 3; ++c) out_x[3 * a + c] = (T)(MODE == 1 ? -x[c] : x[c]);
@@ -179,7 +209,8 @@ __global__ void finalize_grads_kernel(ClusterData<T> cl, const typename Acc<T>::
   }
   if (MODE == 1 && energy && blockIdx.x == 0 && threadIdx.x == 0) {
     const double rec = e_pme ? kc * e_pme[0] : 0.0, self = e_pme ? kc * e_pme[1] : 0.0;
-    energy[0] = Acc<T>::get(&e_tile[0]) + Acc<T>::get(&e_tile[1]) + rec + self;
+    const double eb = bonded ? Acc<T>::get(&bonded[3 * cl.natoms]) + Acc<T>::get(&bonded[3 * cl.natoms + 1]) : 0.0;
+    energy[0] = Acc<T>::get(&e_tile[0]) + Acc<T>::get(&e_tile[1]) + rec + self + eb;
   }
 }
 
@@ -191,11 +222,19 @@ int system_grad_impl(tff_system sys, const T *x, const T *box, const T *dir, dou
                      T *out_s, T *out_e, cudaStream_t s) {
   using S = typename Acc<T>::S;
   const int64_t n = sys->desc.natoms;
+  if (MODE == 2 && sys->has_bonded()) {
+    set_error("second derivatives of the bonded terms are not implemented");
+    return TFF_ERR_INVALID;
+  }
   const int sms = sm_count();
   S *energies = reinterpret_cast<S *>(sys->scratch);
   TFF_CUDA(cudaMemsetAsync(sys->scratch, 0, 8 * sizeof(double), s));
   const bool use_pme = sys->pme && n > 0;
   const double *e_pme = nullptr;
+  if (MODE == 1 && !use_pme && sys->has_bonded() && n > 0) {
+    const int sb = launch_bonded<T>(sys, x, s);
+    if (sb != TFF_OK) return sb;
+  }
   if (use_pme) {
     TFF_CUDA(cudaEventRecord(sys->fork_ev, s));
     TFF_CUDA(cudaStreamWaitEvent(sys->pme_stream, sys->fork_ev, 0));
@@ -205,6 +244,10 @@ int system_grad_impl(tff_system sys, const T *x, const T *box, const T *dir, dou
     char *pw = static_cast<char *>(sys->pme_ws);
     PlainAtoms<T> atoms{x, static_cast<const T *>(sys->q), n};
     T *phi_grid = nullptr;
+    if (MODE == 1 && sys->has_bonded()) {
+      const int sb = launch_bonded<T>(sys, x, ps);
+      if (sb != TFF_OK) return sb;
+    }
     int st = pme_grid_phase<T>(sys->pme->impl, sys->pl, pw, atoms, n, box, sys->desc.ewald_alpha, xm, ym, zm, ps,
                                &phi_grid);
     if (st != TFF_OK) return st;
@@ -269,7 +312,10 @@ int system_grad_impl(tff_system sys, const T *x, const T *box, const T *dir, dou
   const int nbf = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sms * 8));
   finalize_grads_kernel<T, MODE><<<nbf, 256, 0, s>>>(cd, acc, pvec, pscal, static_cast<const T *>(sys->eps),
                                                      sys->desc.coul_constant, out_x, out_q, out_s, out_e, energies,
-                                                     e_pme, energy);
+                                                     e_pme, energy,
+                                                     MODE == 1 && sys->has_bonded() && n > 0
+                                                         ? static_cast<const S *>(sys->bacc)
+                                                         : nullptr);
   TFF_LAUNCHED();
   return TFF_OK;
 }
@@ -294,7 +340,7 @@ void free_system(tff_system sys) {
   void *ptrs[] = {sys->cl_ws, sys->pme_ws, sys->pme_ws2, sys->dir_sorted, sys->pme_hx, sys->pme_hq,
                   sys->acc, sys->lj, sys->exslot, sys->pme_grad, sys->pme_phi,
                   sys->q, sys->sigma, sys->eps, sys->excl, sys->moduli, sys->scratch, sys->host_x,
-                  sys->dev_x, sys->dev_f, sys->dev_e};
+                  sys->dev_x, sys->dev_f, sys->dev_e, sys->bonds, sys->angles, sys->bpar, sys->bacc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete sys;
@@ -422,6 +468,51 @@ int tff_system_create(const tff_system_desc *desc, const double *charges, const 
 
 int tff_system_destroy(tff_system sys) {
   free_system(sys);
+  return TFF_OK;
+}
+
+int tff_system_set_bonded(tff_system sys, int64_t nbonds, const int64_t *bonds, const double *b0, const double *kb,
+                          int64_t nangles, const int64_t *angles, const double *theta0, const double *ktheta) {
+  TFF_ARG(sys != nullptr, "system is NULL");
+  TFF_ARG(nbonds >= 0 && nangles >= 0, "negative sizes");
+  TFF_ARG(nbonds == 0 || (bonds && b0 && kb), "bonds / b0 / kb is NULL");
+  TFF_ARG(nangles == 0 || (angles && theta0 && ktheta), "angles / theta0 / ktheta is NULL");
+  const int64_t n = sys->desc.natoms;
+  for (int64_t m = 0; m < 2 * nbonds; ++m) TFF_ARG(bonds[m] >= 0 && bonds[m] < n, "bond atom index out of range");
+  for (int64_t m = 0; m < 3 * nangles; ++m)
+    TFF_ARG(angles[m] >= 0 && angles[m] < n, "angle atom index out of range");
+  TFF_CUDA(cudaDeviceSynchronize());
+  for (void *p : {(void *)sys->bonds, (void *)sys->angles, sys->bpar, sys->bacc})
+    if (p) cudaFree(p);
+  sys->bonds = sys->angles = nullptr;
+  sys->bpar = sys->bacc = nullptr;
+  sys->nbonds = sys->nangles = 0;
+  if (sys->host_graph) {  // the cached host-path graph does not hold the new terms
+    cudaGraphExecDestroy(sys->host_graph);
+    sys->host_graph = nullptr;
+  }
+  if (nbonds + nangles == 0) return TFF_OK;
+  const size_t ts = sys->desc.dtype == TFF_F64 ? 8 : 4;
+  std::vector<double> par;
+  par.insert(par.end(), b0, b0 + nbonds);
+  par.insert(par.end(), kb, kb + nbonds);
+  par.insert(par.end(), theta0, theta0 + nangles);
+  par.insert(par.end(), ktheta, ktheta + nangles);
+  std::vector<float> parf(par.begin(), par.end());
+  const void *src = ts == 8 ? (const void *)par.data() : (const void *)parf.data();
+  TFF_CUDA(cudaMalloc(&sys->bacc, (3 * n + 2) * 8));
+  TFF_CUDA(cudaMalloc(&sys->bpar, std::max<size_t>(1, par.size()) * ts));
+  TFF_CUDA(cudaMemcpy(sys->bpar, src, par.size() * ts, cudaMemcpyHostToDevice));
+  if (nbonds > 0) {
+    TFF_CUDA(cudaMalloc(&sys->bonds, 2 * nbonds * sizeof(int64_t)));
+    TFF_CUDA(cudaMemcpy(sys->bonds, bonds, 2 * nbonds * sizeof(int64_t), cudaMemcpyHostToDevice));
+  }
+  if (nangles > 0) {
+    TFF_CUDA(cudaMalloc(&sys->angles, 3 * nangles * sizeof(int64_t)));
+    TFF_CUDA(cudaMemcpy(sys->angles, angles, 3 * nangles * sizeof(int64_t), cudaMemcpyHostToDevice));
+  }
+  sys->nbonds = nbonds;
+  sys->nangles = nangles;
   return TFF_OK;
 }
 

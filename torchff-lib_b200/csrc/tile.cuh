@@ -20,6 +20,7 @@
 #include <cmath>
 #include <vector>
 
+#include "bonded.cuh"
 #include "pme.cuh"
 
 namespace tff {
@@ -542,17 +543,25 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
 // Sorted real-space accumulators + caller-order PME derivatives -> caller order; energies
 // of each of the nsys systems (e_tile_acc and e_pme hold two values per system, terms
 // gets four: real-space pairs, exclusion correction, reciprocal, self).
+// With `bonded` (one system): its caller-order dE/dx (3N) and the bond and angle energies
+// (at 3N, 3N + 1) are added too, and terms gets six values (+ bonds, angles).
 template <class T>
 __global__ void finalize_kernel(ClusterData<T> cl, const typename Acc<T>::S *gx, const typename Acc<T>::S *gq,
                                 const T *pme_grad, const T *pme_phi, T *forces, double *forces64, T *grad_q,
                                 const typename Acc<T>::S *e_tile_acc, const double *e_pme, double kc,
-                                double *energy, double *terms, int nsys) {
+                                double *energy, double *terms, int nsys,
+                                const typename Acc<T>::S *bonded = nullptr) {
   pdl_enter();
   for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < cl.natoms;
        a += (int64_t)gridDim.x * blockDim.x) {
     const int64_t s = cl.inv[a];
     double x = Acc<T>::get(&gx[3 * s]), y = Acc<T>::get(&gx[3 * s + 1]), z = Acc<T>::get(&gx[3 * s + 2]);
     double g = Acc<T>::get(&gq[s]);
+    if (bonded) {
+      x += Acc<T>::get(&bonded[3 * a]);
+      y += Acc<T>::get(&bonded[3 * a + 1]);
+      z += Acc<T>::get(&bonded[3 * a + 2]);
+    }
     if (pme_grad) {
       x += kc * (double)pme_grad[3 * a];
       y += kc * (double)pme_grad[3 * a + 1];
@@ -575,13 +584,20 @@ __global__ void finalize_kernel(ClusterData<T> cl, const typename Acc<T>::S *gx,
     const double e_tile[2] = {Acc<T>::get(&e_tile_acc[2 * sy]), Acc<T>::get(&e_tile_acc[2 * sy + 1])};
     const double rec = e_pme ? kc * e_pme[2 * sy] : 0.0;
     const double self = e_pme ? kc * e_pme[2 * sy + 1] : 0.0;
-    const double tot = e_tile[0] + e_tile[1] + rec + self;
+    const double eb = bonded ? Acc<T>::get(&bonded[3 * cl.natoms]) : 0.0;
+    const double ea = bonded ? Acc<T>::get(&bonded[3 * cl.natoms + 1]) : 0.0;
+    const double tot = e_tile[0] + e_tile[1] + rec + self + eb + ea;
     if (energy) energy[sy] = tot;
     if (terms) {
-      terms[4 * sy] = e_tile[0];
-      terms[4 * sy + 1] = e_tile[1];
-      terms[4 * sy + 2] = rec;
-      terms[4 * sy + 3] = self;
+      const int nt = bonded ? 6 : 4;
+      terms[nt * sy] = e_tile[0];
+      terms[nt * sy + 1] = e_tile[1];
+      terms[nt * sy + 2] = rec;
+      terms[nt * sy + 3] = self;
+      if (bonded) {
+        terms[nt * sy + 4] = eb;
+        terms[nt * sy + 5] = ea;
+      }
     }
   }
 }

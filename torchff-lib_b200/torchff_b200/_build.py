@@ -18,7 +18,7 @@ CSRC = os.path.join(ROOT, "csrc")
 INCLUDE = os.path.join(os.path.dirname(ROOT), "include")
 BUILD = os.path.join(ROOT, "_build")
 LIB_NAME = "libtffb200.so"
-SOURCES = ["tff_common.cu", "pairs.cu", "nblist.cu", "cpairs.cu", "pme.cu", "fused.cu", "batch.cu", "server.cu"]
+SOURCES = ["tff_common.cu", "pairs.cu", "nblist.cu", "cpairs.cu", "bonded.cu", "pme.cu", "fused.cu", "batch.cu", "server.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # -ftz=true: FP32 subnormals flush to zero (none arise on this path); FP64 is unaffected

@@ -73,6 +73,12 @@ _SIGS = {
                                           i64, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
     "tff_nonbonded_forces_cluster_pairs": (i32, [i32, i64, vp, vp, vp, vp, vp, f64, f64, vp, i64, vp, i64, vp, vp,
                                                  vp, i64, vp, vp, sz, vp]),
+    "tff_bonded_workspace_bytes": (sz, [i32, i64, i64]),
+    "tff_harmonic_bond": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "tff_harmonic_bond_forces": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, sz, vp]),
+    "tff_harmonic_angle": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "tff_harmonic_angle_forces": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, sz, vp]),
+    "tff_angles": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, sz, vp]),
     "tff_pairs_workspace_bytes": (sz, [i32, i64, i64]),
     "tff_nonbonded_atom_pairs": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, f64, f64, i32, vp, vp, vp, vp, vp,
                                        vp, sz, vp]),
@@ -90,6 +96,7 @@ _SIGS = {
     "tff_pme_long_range": (i32, [vp, i64, vp, vp, vp, f64, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
     "tff_system_create": (i32, [C.POINTER(SystemDesc), vp, vp, vp, i64, vp, C.POINTER(vp)]),
     "tff_system_destroy": (i32, [vp]),
+    "tff_system_set_bonded": (i32, [vp, i64, vp, vp, vp, i64, vp, vp, vp]),
     "tff_system_set_parameters": (i32, [vp, vp, vp, vp, vp]),
     "tff_system_eval": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
     "tff_system_eval_host": (i32, [vp, vp, vp, vp, vp, vp]),

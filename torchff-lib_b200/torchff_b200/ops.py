@@ -43,6 +43,12 @@ SCHEMAS = {
     "decode_cluster_pairs": "decode_cluster_pairs(Tensor coords, Tensor box, Tensor sorted_atom_indices, Tensor cluster_exclusions, Tensor bitmask_exclusions, Tensor interacting_clusters, Tensor interacting_atoms, Scalar cutoff, Scalar max_npairs, bool padding) -> (Tensor, Tensor)",
     "compute_nonbonded_energy_from_cluster_pairs": "compute_nonbonded_energy_from_cluster_pairs(Tensor coords, Tensor box, Tensor sigma, Tensor epsilon, Tensor charges, Tensor coul_constant, Scalar cutoff, Tensor sorted_atom_indices, Tensor cluster_exclusions, Tensor bitmask_exclusions, Tensor interacting_clusters, Tensor interacting_atoms, bool do_shift) -> Tensor",
     "compute_nonbonded_forces_from_cluster_pairs": "compute_nonbonded_forces_from_cluster_pairs(Tensor coords, Tensor box, Tensor sigma, Tensor epsilon, Tensor charges, Tensor coul_constant, Scalar cutoff, Tensor sorted_atom_indices, Tensor cluster_exclusions, Tensor bitmask_exclusions, Tensor interacting_clusters, Tensor interacting_atoms, Tensor forces) -> ()",
+    # bonded terms (csrc/bond/bond_interface.cpp:5-6, csrc/angle/angle_interface.cpp:5-8)
+    "compute_harmonic_bond_energy": "compute_harmonic_bond_energy(Tensor coords, Tensor pairs, Tensor b0, Tensor k) -> Tensor",
+    "compute_harmonic_bond_forces": "compute_harmonic_bond_forces(Tensor coords, Tensor pairs, Tensor b0, Tensor k, Tensor(a!) forces) -> ()",
+    "compute_harmonic_angle_energy": "compute_harmonic_angle_energy(Tensor coords, Tensor angles, Tensor theta0, Tensor k) -> Tensor",
+    "compute_harmonic_angle_forces": "compute_harmonic_angle_forces(Tensor coords, Tensor angles, Tensor theta0, Tensor k, Tensor(a!) forces) -> ()",
+    "compute_angles": "compute_angles(Tensor coords, Tensor angles) -> Tensor",
     "pme_long_range": "pme_long_range(Tensor coords, Tensor box, Tensor q, Tensor? p, Tensor? t, Scalar K, Scalar alpha, Tensor xmoduli, Tensor ymoduli, Tensor zmoduli) -> Tensor",
 }
 for _s in SCHEMAS.values():
@@ -639,3 +645,104 @@ def _pme_cuda(coords, box, q, p, t, K, alpha, xmoduli, ymoduli, zmoduli):
 
 _DEF.impl("pme_long_range", lambda *a: _PmeFn.apply(*a), "AutogradCUDA")
 _DEF.impl("pme_long_range", _pme_cuda, "CUDA")
+
+
+# ---------------------------------------------------------------------------------------
+# bonded terms (AutogradCUDA + CUDA; forces variants CUDA)
+# ---------------------------------------------------------------------------------------
+
+def _bonded_ws(x: torch.Tensor, nterms: int) -> torch.Tensor:
+    return L.workspace(L.lib.tff_bonded_workspace_bytes(L.dtype_code(x.dtype), x.shape[0], nterms), x.device)
+
+
+def bonded_forward(angle: bool, coords, idx, p0, k, need=(False, False, False)):
+    """Energy (0-d) of harmonic bonds (angle=False) or angles and the optional dE/dx,
+    dE/dp0, dE/dk (``need`` in that order)."""
+    L.require_cuda(coords, idx, p0, k)
+    x = _c(coords.detach())
+    dt = x.dtype
+    ix = _long(idx.detach())
+    if ix.dim() != 2 or ix.shape[1] != (3 if angle else 2):
+        raise RuntimeError(f"{'angles' if angle else 'bonds'} must be an (M, {3 if angle else 2}) index tensor")
+    a, kk = _c(p0.detach(), dt), _c(k.detach(), dt)
+    ene = torch.empty((), dtype=dt, device=x.device)
+    gx = _empty_like_or_none(x, need[0])
+    gp = _empty_like_or_none(a, need[1])
+    gk = _empty_like_or_none(kk, need[2])
+    ws = _bonded_ws(x, ix.shape[0])
+    fn = L.lib.tff_harmonic_angle if angle else L.lib.tff_harmonic_bond
+    L.check(fn(L.dtype_code(dt), x.shape[0], L.ptr(x), ix.shape[0], L.ptr(ix), L.ptr(a), L.ptr(kk), L.ptr(ene),
+               L.ptr(gx), L.ptr(gp), L.ptr(gk), L.ptr(ws), ws.numel(), L.stream_of(x)),
+            "compute_harmonic_angle_energy" if angle else "compute_harmonic_bond_energy")
+    return ene, gx, gp, gk
+
+
+class _BondedFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, angle, coords, idx, p0, k):
+        ni = ctx.needs_input_grad
+        ene, gx, gp, gk = bonded_forward(angle, coords, idx, p0, k, (ni[1], ni[3], ni[4]))
+        ctx.save_for_backward(gx, gp, gk)
+        return ene
+
+    @staticmethod
+    def backward(ctx, g):
+        gx, gp, gk = ctx.saved_tensors
+        sc = lambda t: None if t is None else t * g
+        return None, sc(gx), None, sc(gp), sc(gk)
+
+
+def _bonded_forces(angle: bool, coords, idx, p0, k, forces):
+    L.require_cuda(coords, idx, p0, k, forces)
+    x = _c(coords.detach())
+    dt = x.dtype
+    if forces.dtype != dt or not forces.is_contiguous() or forces.shape != x.shape:
+        raise RuntimeError("forces must be a contiguous tensor shaped and typed like coords")
+    ix = _long(idx.detach())
+    a, kk = _c(p0.detach(), dt), _c(k.detach(), dt)
+    ws = _bonded_ws(x, ix.shape[0])
+    fn = L.lib.tff_harmonic_angle_forces if angle else L.lib.tff_harmonic_bond_forces
+    L.check(fn(L.dtype_code(dt), x.shape[0], L.ptr(x), ix.shape[0], L.ptr(ix), L.ptr(a), L.ptr(kk), L.ptr(forces),
+               L.ptr(ws), ws.numel(), L.stream_of(x)),
+            "compute_harmonic_angle_forces" if angle else "compute_harmonic_bond_forces")
+
+
+def _angles_run(coords, angles, grad_theta=None):
+    x = _c(coords.detach())
+    ix = _long(angles.detach())
+    if ix.dim() != 2 or ix.shape[1] != 3:
+        raise RuntimeError("angles must be an (M, 3) index tensor")
+    if grad_theta is None:
+        theta = torch.empty(ix.shape[0], dtype=x.dtype, device=x.device)
+        L.check(L.lib.tff_angles(L.dtype_code(x.dtype), x.shape[0], L.ptr(x), ix.shape[0], L.ptr(ix), L.ptr(theta),
+                                 None, None, None, 0, L.stream_of(x)), "compute_angles")
+        return theta
+    gt = _c(grad_theta.detach(), x.dtype)
+    gx = torch.empty_like(x)
+    ws = _bonded_ws(x, ix.shape[0])
+    L.check(L.lib.tff_angles(L.dtype_code(x.dtype), x.shape[0], L.ptr(x), ix.shape[0], L.ptr(ix), None, L.ptr(gt),
+                             L.ptr(gx), L.ptr(ws), ws.numel(), L.stream_of(x)), "compute_angles backward")
+    return gx
+
+
+class _AnglesFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coords, angles):
+        L.require_cuda(coords, angles)
+        ctx.save_for_backward(coords, angles)
+        return _angles_run(coords, angles)
+
+    @staticmethod
+    def backward(ctx, g):
+        coords, angles = ctx.saved_tensors
+        return _angles_run(coords, angles, g), None
+
+
+_DEF.impl("compute_harmonic_bond_energy", lambda *a: _BondedFn.apply(False, *a), "AutogradCUDA")
+_DEF.impl("compute_harmonic_bond_energy", lambda *a: bonded_forward(False, *a)[0], "CUDA")
+_DEF.impl("compute_harmonic_bond_forces", lambda *a: _bonded_forces(False, *a), "CUDA")
+_DEF.impl("compute_harmonic_angle_energy", lambda *a: _BondedFn.apply(True, *a), "AutogradCUDA")
+_DEF.impl("compute_harmonic_angle_energy", lambda *a: bonded_forward(True, *a)[0], "CUDA")
+_DEF.impl("compute_harmonic_angle_forces", lambda *a: _bonded_forces(True, *a), "CUDA")
+_DEF.impl("compute_angles", lambda c, a: _AnglesFn.apply(c, a), "AutogradCUDA")
+_DEF.impl("compute_angles", lambda c, a: (L.require_cuda(c, a), _angles_run(c, a))[1], "CUDA")

@@ -58,10 +58,41 @@ class FixedChargeSystem:
                          (("charges", q), ("sigma", s), ("epsilon", e))}
 
     @classmethod
-    def from_water_box(cls, wb, dtype=torch.float32, device="cuda", **kw):
-        """System for a ``torchff_b200.water.WaterBox`` (TIP3P parameters and exclusions)."""
-        return cls(wb.charges, wb.sigma, wb.epsilon, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
+    def from_water_box(cls, wb, dtype=torch.float32, device="cuda", flexible: bool = False, **kw):
+        """System for a ``torchff_b200.water.WaterBox`` (TIP3P parameters and exclusions);
+        ``flexible`` adds the harmonic O-H bonds and H-O-H angles of flexible TIP3P."""
+        sys_ = cls(wb.charges, wb.sigma, wb.epsilon, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
                    dtype=dtype, device=device, **kw)
+        if flexible:
+            from .water import water_bonded_terms
+            bt = water_bonded_terms(wb.n_waters)
+            sys_.set_bonded(bt.bonds, bt.b0, bt.kb, bt.angles, bt.th0, bt.kth)
+        return sys_
+
+    def set_bonded(self, bonds=None, b0=None, kb=None, angles=None, theta0=None, ktheta=None) -> None:
+        """Harmonic bonds (M,2) with b0, kb and angles (M,3) with theta0, ktheta (central atom
+        in the middle) evaluated with the nonbonded terms (examples/tip3p/model.py:105-106).
+        All None removes them. Synchronises the device."""
+        def arr(a, dt, shape=None):
+            a = np.ascontiguousarray(np.asarray(a.detach().cpu() if isinstance(a, torch.Tensor) else a, dtype=dt))
+            return a if shape is None else a.reshape(shape)
+        nb = na = 0
+        bd = b0a = kba = an = t0a = kta = None
+        if bonds is not None:
+            bd = arr(bonds, np.int64, (-1, 2)); b0a = arr(b0, np.float64, -1); kba = arr(kb, np.float64, -1)
+            nb = bd.shape[0]
+            if b0a.shape[0] != nb or kba.shape[0] != nb:
+                raise ValueError("b0 and kb need one value per bond")
+        if angles is not None:
+            an = arr(angles, np.int64, (-1, 3)); t0a = arr(theta0, np.float64, -1); kta = arr(ktheta, np.float64, -1)
+            na = an.shape[0]
+            if t0a.shape[0] != na or kta.shape[0] != na:
+                raise ValueError("theta0 and ktheta need one value per angle")
+        p = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+        with torch.cuda.device(self.device):
+            L.check(L.lib.tff_system_set_bonded(self._h, nb, p(bd), p(b0a), p(kba), na, p(an), p(t0a), p(kta)),
+                    "tff_system_set_bonded")
+        self.nbonded_terms = nb + na
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -87,7 +118,8 @@ class FixedChargeSystem:
 
         coords (N,3) and box (3,3) in the system dtype; energy: float64 (1,); forces (N,3)
         system dtype (= -dE/dx); grad_charges (N,) dE/dq; energy_terms float64 (4,):
-        real-space pairs, exclusion correction, reciprocal, self.
+        real-space pairs, exclusion correction, reciprocal, self; (6,) with bonded terms
+        (then bonds, angles).
         """
         L.check(L.lib.tff_system_eval(self._h, L.ptr(coords), L.ptr(box), L.ptr(energy), L.ptr(forces),
                                       L.ptr(grad_charges), L.ptr(energy_terms), self._stream()), "tff_system_eval")
@@ -100,7 +132,8 @@ class FixedChargeSystem:
         energy = torch.empty(1, dtype=torch.float64, device=self.device)
         forces = torch.empty_like(x)
         gq = torch.empty(self.natoms, dtype=self.dtype, device=self.device) if grad_charges else None
-        et = torch.empty(4, dtype=torch.float64, device=self.device) if terms else None
+        et = torch.empty(6 if getattr(self, "nbonded_terms", 0) else 4, dtype=torch.float64,
+                         device=self.device) if terms else None
         self.evaluate_into(x, b, energy, forces, gq, et)
         out = {"energy": energy[0], "forces": forces}
         if gq is not None:

@@ -92,6 +92,32 @@ def water_exclusions(n_waters: int) -> tuple[np.ndarray, np.ndarray]:
     return nb.astype(np.int64), coul.astype(np.int64)
 
 
+# Flexible TIP3P bonded parameters (the harmonic terms of OpenMM's tip3p-flexible force field):
+# E_bond = 1/2 K_BOND (r - OH_BOND)^2, E_angle = 1/2 K_ANGLE (theta - HOH_ANGLE)^2.
+K_BOND = 462750.4        # kJ mol^-1 nm^-2
+K_ANGLE = 836.8          # kJ mol^-1 rad^-2
+
+
+@dataclass
+class WaterBonded:
+    bonds: np.ndarray    # (2 n, 2) int64: O-H1, O-H2 per water
+    b0: np.ndarray       # (2 n,) nm
+    kb: np.ndarray       # (2 n,) kJ/mol/nm^2
+    angles: np.ndarray   # (n, 3) int64: H1-O-H2 (O central)
+    th0: np.ndarray      # (n,) rad
+    kth: np.ndarray      # (n,) kJ/mol/rad^2
+
+
+def water_bonded_terms(n_waters: int) -> WaterBonded:
+    """Harmonic O-H bonds and H-O-H angles of n flexible TIP3P waters (atoms O, H1, H2)."""
+    base = 3 * np.arange(n_waters, dtype=np.int64)
+    bonds = np.stack([np.stack([base, base + 1], 1), np.stack([base, base + 2], 1)], 1).reshape(-1, 2)
+    angles = np.stack([base + 1, base, base + 2], 1)
+    return WaterBonded(bonds=bonds, b0=np.full(2 * n_waters, OH_BOND), kb=np.full(2 * n_waters, K_BOND),
+                       angles=angles, th0=np.full(n_waters, math.radians(HOH_ANGLE_DEG)),
+                       kth=np.full(n_waters, K_ANGLE))
+
+
 def make_water_box(
     n_waters: int,
     box_len: float,
