@@ -36,6 +36,39 @@ def lib_path() -> str:
     return os.path.join(PKG_DIR, LIB_NAME)
 
 
+# TorchScript binding for C++ hosts (torch.classes.torchff_b200.System), linked against
+# libtffb200.so and libtorch; built with the host C++ compiler.
+TORCH_LIB_NAME = "libtffb200_torch.so"
+TORCH_SHIM = "torch_shim.cpp"
+
+
+def torch_lib_path() -> str:
+    return os.path.join(PKG_DIR, TORCH_LIB_NAME)
+
+
+def build_torch_shim(force: bool = False) -> str:
+    import torch.utils.cpp_extension as ce
+
+    src = os.path.join(CSRC, TORCH_SHIM)
+    out = torch_lib_path()
+    deps = [src, os.path.join(INCLUDE, "tffb200.h"), lib_path()]
+    if not force and os.path.exists(out) and not _needs_rebuild(out, deps):
+        return out
+    import torch
+
+    cuda = os.path.dirname(os.path.dirname(nvcc()))
+    tlib = ce.library_paths()[0]
+    cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", "-fPIC", "-shared",
+           f"-D_GLIBCXX_USE_CXX11_ABI={int(torch._C._GLIBCXX_USE_CXX11_ABI)}",
+           *[f"-I{p}" for p in ce.include_paths()], f"-I{os.path.join(cuda, 'include')}", f"-I{INCLUDE}",
+           src, "-o", out, f"-L{tlib}", "-ltorch", "-ltorch_cpu", "-lc10", "-lc10_cuda", f"-L{PKG_DIR}", "-ltffb200",
+           "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{tlib}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"g++ failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return out
+
+
 def _needs_rebuild(obj: str, deps: list[str]) -> bool:
     if not os.path.exists(obj):
         return True
@@ -73,6 +106,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         link = [nvcc(), *ARCH, "-shared", "-o", out, *objs, "-cudart", "static", "-lcufft",
                 "-L", os.path.join(cuda, "lib64"), "-Xlinker", f"-rpath,{os.path.join(cuda, 'lib64')}"]
         run(link)
+    build_torch_shim(force)
     return out
 
 
