@@ -354,7 +354,10 @@ int tff_system_set_bonded(tff_system sys, int64_t nbonds, const int64_t *bonds, 
 int tff_system_eval(tff_system sys, const void *coords, const void *box, double *energy,
                     void *forces, void *grad_charges, double *energy_terms, tff_stream_t stream);
 /* Same with HOST buffers: copies coords/box in, evaluates, copies energy/forces out and
- * synchronises `stream`. coords/box/forces are float64 host arrays whatever the dtype. */
+ * synchronises `stream`. coords/box/forces are float64 host arrays whatever the dtype.
+ * When coords and forces are page-locked (cudaHostAlloc / cudaHostRegister) the copies and
+ * the evaluation are one CUDA-graph launch, kept for the last (coords, forces) pair seen and
+ * captured again when either pointer changes. */
 int tff_system_eval_host(tff_system sys, const double *coords, const double *box,
                          double *energy, double *forces, tff_stream_t stream);
 /* Device status word of the last evaluation (bit 0: a cluster neighbour list overflowed,

@@ -121,6 +121,28 @@ def test_host_entry_point_matches_device(ref216):
             assert rel_max(f, dev["forces"]) < 1e-12
 
 
+def test_host_entry_point_page_locked_buffers(ref216):
+    """Page-locked coords/forces take the one-graph path (copies inside the graph): results equal
+    the device path on consecutive calls with new coordinates, on a second pair of buffers, and
+    when the box is not page-locked."""
+    from torchff_b200.system import FixedChargeSystem
+
+    wb, _ = ref216
+    sysm = FixedChargeSystem.from_water_box(wb, dtype=torch.float32)
+    rng = np.random.default_rng(4)
+    bufs = [(torch.empty((wb.natoms, 3), dtype=torch.float64).pin_memory(),
+             torch.empty((wb.natoms, 3), dtype=torch.float64).pin_memory()) for _ in range(2)]
+    box = np.ascontiguousarray(wb.box)
+    for step in range(4):
+        hx, hf = bufs[step // 2]
+        x = wb.coords + rng.normal(0.0, 0.003, wb.coords.shape)
+        hx.copy_(torch.from_numpy(x))
+        e = sysm.evaluate_host(hx, box, hf)
+        dev = sysm.evaluate(t(x, torch.float32), t(wb.box, torch.float32))
+        assert e == dev["energy"].item()
+        assert np.array_equal(hf.numpy().astype(np.float32), dev["forces"].cpu().numpy())
+
+
 def test_cuda_graph_replay_matches_eager(ref3000):
     from torchff_b200.system import FixedChargeSystem
 

@@ -47,6 +47,11 @@ struct tff_system_s {
   double *dev_e = nullptr;
   cudaGraphExec_t host_graph = nullptr;  // device part of tff_system_eval_host, captured once
   cudaStream_t capture_stream = nullptr;
+  // tff_system_eval_host with page-locked caller buffers: one graph that also holds the
+  // copies, for the last (coords, box, energy, forces) pointers seen
+  cudaGraphExec_t pinned_graph = nullptr;
+  const void *pinned_ptrs[2] = {nullptr, nullptr};
+  double *pinned_io = nullptr;  // page-locked: box (9) in, energy (1) out
   // bonded terms (flexible water), set by tff_system_set_bonded
   int64_t nbonds = 0, nangles = 0;
   int64_t *bonds = nullptr, *angles = nullptr;  // (M,2), (M,3)
@@ -336,6 +341,8 @@ void free_system(tff_system sys) {
   if (sys->fork_ev) cudaEventDestroy(sys->fork_ev);
   if (sys->join_ev) cudaEventDestroy(sys->join_ev);
   if (sys->host_graph) cudaGraphExecDestroy(sys->host_graph);
+  if (sys->pinned_graph) cudaGraphExecDestroy(sys->pinned_graph);
+  if (sys->pinned_io) cudaFreeHost(sys->pinned_io);
   if (sys->capture_stream) cudaStreamDestroy(sys->capture_stream);
   void *ptrs[] = {sys->cl_ws, sys->pme_ws, sys->pme_ws2, sys->dir_sorted, sys->pme_hx, sys->pme_hq,
                   sys->acc, sys->lj, sys->exslot, sys->pme_grad, sys->pme_phi,
@@ -487,9 +494,13 @@ int tff_system_set_bonded(tff_system sys, int64_t nbonds, const int64_t *bonds, 
   sys->bonds = sys->angles = nullptr;
   sys->bpar = sys->bacc = nullptr;
   sys->nbonds = sys->nangles = 0;
-  if (sys->host_graph) {  // the cached host-path graph does not hold the new terms
+  if (sys->host_graph) {  // the cached host-path graphs do not hold the new terms
     cudaGraphExecDestroy(sys->host_graph);
     sys->host_graph = nullptr;
+  }
+  if (sys->pinned_graph) {
+    cudaGraphExecDestroy(sys->pinned_graph);
+    sys->pinned_graph = nullptr;
   }
   if (nbonds + nangles == 0) return TFF_OK;
   const size_t ts = sys->desc.dtype == TFF_F64 ? 8 : 4;
@@ -538,24 +549,30 @@ int tff_system_eval(tff_system sys, const void *coords, const void *box, double 
                                   (double *)grad_charges, energy_terms, s);
 }
 
-int tff_system_eval_host(tff_system sys, const double *coords, const double *box, double *energy, double *forces,
-                         tff_stream_t stream) {
-  TFF_ARG(sys != nullptr, "system is NULL");
-  TFF_ARG(box != nullptr && energy != nullptr, "box/energy is NULL");
+}  // extern "C"
+
+namespace {
+
+// Captures the device part of tff_system_eval_host (FP64 -> system dtype cast of the staged
+// coordinates and box, evaluation into internal buffers). With `coords` / `forces` (page-locked
+// host buffers of the caller) the graph also holds the copies: coordinates in, box in from the
+// system's page-locked box slot, forces out, energy out to the system's page-locked energy slot.
+int capture_host_graph(tff_system sys, const double *coords, double *forces, cudaGraphExec_t *out) {
   const int64_t n = sys->desc.natoms;
-  TFF_ARG(n == 0 || (coords != nullptr && forces != nullptr), "coords/forces is NULL");
-  cudaStream_t s = (cudaStream_t)stream;
   double *stage = static_cast<double *>(sys->host_x);
-  // The device part (FP64 -> system dtype cast + evaluation into internal buffers) only
-  // touches the system's own buffers, so it is captured into a CUDA graph on the first
-  // call (on an internal stream) and replayed on `stream` afterwards.
-  if (sys->host_graph == nullptr) {
-    if (sys->capture_stream == nullptr)
-      TFF_CUDA(cudaStreamCreateWithFlags(&sys->capture_stream, cudaStreamNonBlocking));
-    cudaStream_t cs = sys->capture_stream;
-    TFF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    int st;
-    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((3 * n + 255) / 256, sm_count() * 8));
+  if (sys->capture_stream == nullptr)
+    TFF_CUDA(cudaStreamCreateWithFlags(&sys->capture_stream, cudaStreamNonBlocking));
+  cudaStream_t cs = sys->capture_stream;
+  TFF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  int st = TFF_OK;
+  cudaError_t ce = cudaSuccess;
+  if (coords) {
+    if (n > 0) ce = cudaMemcpyAsync(stage, coords, 3 * n * sizeof(double), cudaMemcpyHostToDevice, cs);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(stage + 3 * n, sys->pinned_io, 9 * sizeof(double), cudaMemcpyHostToDevice, cs);
+  }
+  const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((3 * n + 255) / 256, sm_count() * 8));
+  if (ce == cudaSuccess) {
     if (sys->desc.dtype == TFF_F32) {
       float *x = static_cast<float *>(sys->dev_x);
       cast_inputs_kernel<float><<<nb, 256, 0, cs>>>(stage, stage + 3 * n, x, x + 3 * n, 3 * n);
@@ -565,19 +582,75 @@ int tff_system_eval_host(tff_system sys, const double *coords, const double *box
       cast_inputs_kernel<double><<<nb, 256, 0, cs>>>(stage, stage + 3 * n, x, x + 3 * n, 3 * n);
       st = system_eval_impl<double>(sys, x, x + 3 * n, sys->dev_e, nullptr, sys->dev_f, nullptr, nullptr, cs);
     }
-    cudaGraph_t graph = nullptr;
-    const cudaError_t ce = cudaStreamEndCapture(cs, &graph);
-    if (st != TFF_OK) {
-      if (graph) cudaGraphDestroy(graph);
-      return st;
+  }
+  if (coords && st == TFF_OK && ce == cudaSuccess) {
+    if (n > 0) ce = cudaMemcpyAsync(forces, sys->dev_f, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, cs);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(sys->pinned_io + 9, sys->dev_e, sizeof(double), cudaMemcpyDeviceToHost, cs);
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(cs, &graph);
+  if (st != TFF_OK || ce != cudaSuccess || ee != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    if (st != TFF_OK) return st;
+    return cuda_fail(ce != cudaSuccess ? ce : ee, "host-path graph capture", __FILE__, __LINE__);
+  }
+  const cudaError_t ie = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) {
+    *out = nullptr;
+    return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+  }
+  return TFF_OK;
+}
+
+bool page_locked(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tff_system_eval_host(tff_system sys, const double *coords, const double *box, double *energy, double *forces,
+                         tff_stream_t stream) {
+  TFF_ARG(sys != nullptr, "system is NULL");
+  TFF_ARG(box != nullptr && energy != nullptr, "box/energy is NULL");
+  const int64_t n = sys->desc.natoms;
+  TFF_ARG(n == 0 || (coords != nullptr && forces != nullptr), "coords/forces is NULL");
+  cudaStream_t s = (cudaStream_t)stream;
+  double *stage = static_cast<double *>(sys->host_x);
+  // Page-locked coordinate and force buffers (the usual case of a caller that reuses them):
+  // one graph launch does copies and evaluation; it is re-captured when the pointers change.
+  const bool pinned = n > 0 && page_locked(coords) && page_locked(forces);
+  if (pinned && (sys->pinned_graph == nullptr || sys->pinned_ptrs[0] != coords || sys->pinned_ptrs[1] != forces)) {
+    if (sys->pinned_io == nullptr) TFF_CUDA(cudaMallocHost(&sys->pinned_io, 16 * sizeof(double)));
+    if (sys->pinned_graph) {
+      cudaGraphExecDestroy(sys->pinned_graph);
+      sys->pinned_graph = nullptr;
     }
-    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
-    const cudaError_t ie = cudaGraphInstantiate(&sys->host_graph, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ie != cudaSuccess) {
-      sys->host_graph = nullptr;
-      return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
-    }
+    const int st = capture_host_graph(sys, coords, forces, &sys->pinned_graph);
+    if (st != TFF_OK) return st;
+    sys->pinned_ptrs[0] = coords;
+    sys->pinned_ptrs[1] = forces;
+  }
+  if (pinned) {
+    std::memcpy(sys->pinned_io, box, 9 * sizeof(double));
+    TFF_CUDA(cudaGraphLaunch(sys->pinned_graph, s));
+    TFF_CUDA(cudaStreamSynchronize(s));
+    *energy = sys->pinned_io[9];
+    return TFF_OK;
+  }
+  // Other buffers: the device part is captured once (it touches only the system's own
+  // buffers) and the copies are issued around it.
+  if (sys->host_graph == nullptr) {
+    const int st = capture_host_graph(sys, nullptr, nullptr, &sys->host_graph);
+    if (st != TFF_OK) return st;
   }
   if (n > 0) TFF_CUDA(cudaMemcpyAsync(stage, coords, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
   TFF_CUDA(cudaMemcpyAsync(stage + 3 * n, box, 9 * sizeof(double), cudaMemcpyHostToDevice, s));
