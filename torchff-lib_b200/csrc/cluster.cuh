@@ -273,10 +273,19 @@ static __global__ void scan_keys_kernel(unsigned *hist, int64_t nkeys) {
   pdl_enter();
   __shared__ unsigned s_warp[32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t per = (nkeys + blockDim.x - 1) / blockDim.x;
+  // segments of whole 4-key chunks read as uint4 (hist is 16-byte aligned), several loads in
+  // flight per thread
+  const int64_t per = ((nkeys + blockDim.x - 1) / blockDim.x + 3) & ~int64_t(3);
   const int64_t beg = min((int64_t)threadIdx.x * per, nkeys), end = min(beg + per, nkeys);
+  const int64_t vend = beg + ((end - beg) & ~int64_t(3));
+  const uint4 *h4 = reinterpret_cast<const uint4 *>(hist);
   unsigned sum = 0;
-  for (int64_t k = beg; k < end; ++k) sum += hist[k];
+#pragma unroll 4
+  for (int64_t k = beg; k < vend; k += 4) {
+    const uint4 v = h4[k >> 2];
+    sum += v.x + v.y + v.z + v.w;
+  }
+  for (int64_t k = vend; k < end; ++k) sum += hist[k];
   unsigned incl = sum;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -297,7 +306,22 @@ static __global__ void scan_keys_kernel(unsigned *hist, int64_t nkeys) {
   }
   __syncthreads();
   unsigned run = s_warp[w] + incl - sum;
-  for (int64_t k = beg; k < end; ++k) {
+  uint4 *o4 = reinterpret_cast<uint4 *>(hist);
+#pragma unroll 4
+  for (int64_t k = beg; k < vend; k += 4) {
+    const uint4 v = h4[k >> 2];
+    uint4 o;
+    o.x = run;
+    run += v.x;
+    o.y = run;
+    run += v.y;
+    o.z = run;
+    run += v.z;
+    o.w = run;
+    run += v.w;
+    o4[k >> 2] = o;
+  }
+  for (int64_t k = vend; k < end; ++k) {
     const unsigned v = hist[k];
     hist[k] = run;
     run += v;
@@ -621,6 +645,40 @@ __device__ __forceinline__ bool clusters_may_interact(const typename V4<T>::type
   return m <= rc;
 }
 
+// The same test in FP32 for float boxes: the box facts of the system are converted once
+// (box diagonal for orthorhombic boxes, perpendicular widths otherwise) and the margin is
+// 2e-6 in fractional units, above the FP32 rounding of centres, extents and the arithmetic
+// (a few 1e-7), so the test stays conservative.
+struct BoxTestF {
+  float s[3];  // orthorhombic: box lengths; otherwise perpendicular widths
+  float lim;   // orthorhombic: rc^2 (1 + 1e-6); otherwise rc (1 + 1e-6)
+  bool ortho;
+};
+
+__device__ __forceinline__ BoxTestF box_test_f(const double *info, double rc) {
+  BoxTestF b;
+  b.ortho = info[18] != 0.0;
+  b.s[0] = (float)(b.ortho ? info[0] : info[19]);
+  b.s[1] = (float)(b.ortho ? info[4] : info[20]);
+  b.s[2] = (float)(b.ortho ? info[8] : info[21]);
+  b.lim = (float)(b.ortho ? rc * rc * (1.0 + 1e-6) : rc * (1.0 + 1e-6));
+  return b;
+}
+
+__device__ __forceinline__ bool boxes_may_interact_f(const float4 &ci, const float4 &hi, const float4 &cj,
+                                                     const float4 &hj, const BoxTestF &b) {
+  const float dc[3] = {ci.x - cj.x, ci.y - cj.y, ci.z - cj.z};
+  const float hs[3] = {hi.x + hj.x, hi.y + hj.y, hi.z + hj.z};
+  float g[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float v = dc[k] - floorf(dc[k] + 0.5f);
+    g[k] = fmaxf(0.f, fabsf(v) - hs[k] - 2e-6f) * b.s[k];
+  }
+  if (b.ortho) return g[0] * g[0] + g[1] * g[1] + g[2] * g[2] <= b.lim;
+  return fmaxf(g[0], fmaxf(g[1], g[2])) <= b.lim;
+}
+
 template <class T>
 __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) {
   pdl_enter();
@@ -641,20 +699,28 @@ __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) 
       s0 = b.sup_off;
     }
     const double *info = d.info(sy);
+    BoxTestF bt{};
+    if constexpr (sizeof(T) == 4) bt = box_test_f(info, rc);
+    auto test = [&](const typename V4<T>::type &cj, const typename V4<T>::type &hj) {
+      if constexpr (sizeof(T) == 4)
+        return boxes_may_interact_f(ci, hi, cj, hj, bt);
+      else
+        return clusters_may_interact<T>(ci, hi, cj, hj, info, rc);
+    };
     const int64_t jend = half ? (I + 1) : j1;
     const int64_t send = s0 + (jend - j0 + kSuper - 1) / kSuper;
     // Lanes screen 32 super-clusters at a time; the members of each survivor (one per lane,
     // kSuper == kWarp) are then tested in ascending order, so the list is sorted by J.
     for (int64_t sb = s0; sb < send; sb += kWarp) {
       const int64_t S = sb + lane;
-      const bool sok = S < send && clusters_may_interact<T>(ci, hi, d.sbc[S], d.sbh[S], info, rc);
+      const bool sok = S < send && test(d.sbc[S], d.sbh[S]);
       unsigned sm = __ballot_sync(kFull, sok);
       while (sm) {
         const int k = __ffs(sm) - 1;
         sm &= sm - 1u;
         const int64_t J = j0 + (sb + k - s0) * kSuper + lane;
         bool ok = false;
-        if (J < jend) ok = clusters_may_interact<T>(ci, hi, d.bc[J], d.bh[J], info, rc);
+        if (J < jend) ok = test(d.bc[J], d.bh[J]);
         const unsigned mm = __ballot_sync(kFull, ok);
         if (ok) {
           const int r = count + __popc(mm & ((1u << lane) - 1u));
