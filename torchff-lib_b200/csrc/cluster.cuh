@@ -710,23 +710,42 @@ __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) 
     const int64_t jend = half ? (I + 1) : j1;
     const int64_t send = s0 + (jend - j0 + kSuper - 1) / kSuper;
     // Lanes screen 32 super-clusters at a time; the members of each survivor (one per lane,
-    // kSuper == kWarp) are then tested in ascending order, so the list is sorted by J.
+    // kSuper == kWarp) are then tested in ascending order, so the list is sorted by J. The
+    // member boxes of up to kBatch survivors are loaded before any of them is tested, so a
+    // warp waits for one round of loads per kBatch survivors rather than per survivor.
+    constexpr int kBatch = 4;
+    using V = typename V4<T>::type;
     for (int64_t sb = s0; sb < send; sb += kWarp) {
       const int64_t S = sb + lane;
       const bool sok = S < send && test(d.sbc[S], d.sbh[S]);
       unsigned sm = __ballot_sync(kFull, sok);
       while (sm) {
-        const int k = __ffs(sm) - 1;
-        sm &= sm - 1u;
-        const int64_t J = j0 + (sb + k - s0) * kSuper + lane;
-        bool ok = false;
-        if (J < jend) ok = test(d.bc[J], d.bh[J]);
-        const unsigned mm = __ballot_sync(kFull, ok);
-        if (ok) {
-          const int r = count + __popc(mm & ((1u << lane) - 1u));
-          if (r < d.cap) d.nbr[I * d.cap + r] = (int)J;
+        int64_t Jb[kBatch];
+        V cb[kBatch], hb[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+          Jb[u] = -1;
+          if (sm) {
+            const int k = __ffs(sm) - 1;
+            sm &= sm - 1u;
+            const int64_t J = j0 + (sb + k - s0) * kSuper + lane;
+            if (J < jend) {
+              Jb[u] = J;
+              cb[u] = d.bc[J];
+              hb[u] = d.bh[J];
+            }
+          }
         }
-        count += __popc(mm);
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+          const bool ok = Jb[u] >= 0 && test(cb[u], hb[u]);
+          const unsigned mm = __ballot_sync(kFull, ok);
+          if (ok) {
+            const int r = count + __popc(mm & ((1u << lane) - 1u));
+            if (r < d.cap) d.nbr[I * d.cap + r] = (int)Jb[u];
+          }
+          count += __popc(mm);
+        }
       }
     }
     if (lane == 0) {
@@ -736,6 +755,7 @@ __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) 
   }
   // The last block to finish turns the counts into work-item offsets (exclusive prefix
   // sums of ceil(count / kItemTiles)); status[1] is the block ticket (zeroed per build).
+  // The item -> cluster table is filled by the sorted-parameter kernel that follows.
   __shared__ bool s_last;
   __shared__ int s_warp[32];
   __syncthreads();
@@ -774,9 +794,7 @@ __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) 
   int run = s_warp[w] + incl - sum;
   for (int64_t k = beg; k < end; ++k) {
     d.itemoff[k] = run;
-    const int nk = (__ldcg(&d.ncount[k]) + kItemTiles - 1) / kItemTiles;
-    for (int j = 0; j < nk; ++j) d.items[run + j] = (int)k;
-    run += nk;
+    run += (__ldcg(&d.ncount[k]) + kItemTiles - 1) / kItemTiles;
   }
   if (threadIdx.x == blockDim.x - 1) d.itemoff[n] = run;
 }

@@ -158,6 +158,12 @@ template <> struct Acc<double> {
   static __device__ __forceinline__ double get(const S *p) { return *p; }
 };
 
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
 // ---------------------------------------------------------------------------------
 // deterministic reductions
 // ---------------------------------------------------------------------------------

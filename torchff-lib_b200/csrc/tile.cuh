@@ -75,6 +75,8 @@ struct TileArgs {
 // With `dir` (caller order (N,3)) also the direction of a second-derivative pass in
 // sorted order.
 // With `gx` / `gq` also zeroes the tile kernel's accumulators of each slot (3 + 1 values).
+// Also fills the tile kernel's item -> cluster table from the item offsets of the
+// neighbour search (the lanes of cluster k write its entries).
 template <class T>
 __global__ void sorted_params_kernel(ClusterData<T> cl, const T *sigma, const T *eps, const int *excl,
                                      typename V2<T>::type *lj, int *exslot, const T *dir = nullptr,
@@ -87,6 +89,11 @@ __global__ void sorted_params_kernel(ClusterData<T> cl, const T *sigma, const T 
       gx[3 * s + 1] = 0;
       gx[3 * s + 2] = 0;
       gq[s] = 0;
+    }
+    {
+      const int64_t k = s / kWarp;
+      const int o = cl.itemoff[k], nk = cl.itemoff[k + 1] - o;
+      for (int j = (int)(s % kWarp); j < nk; j += kWarp) cl.items[o + j] = (int)k;
     }
     const int a = cl.sidx[s];
     if (dir)
@@ -135,6 +142,7 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
   __shared__ unsigned s_xmask[NW][kItemTiles][kWarp];  // in-cutoff, excluded
   __shared__ int s_mi[NW][kItemTiles];                 // 1: tile needs the per-pair minimum image
   __shared__ T s_box[NW][2][9];                         // box and inverse of the warp's current system
+  __shared__ T s_rpre2[NW];                             // squared j-atom prefilter radius of that system
   const ClusterData<T> &cl = A.cl;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   T *s_m = s_box[w][0], *s_inv = s_box[w][1];
@@ -159,6 +167,10 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
       }
       ortho = info[18] != 0.0;
       cur_sys = isys;
+      if (lane == 0) {
+        const T rpre = (T)(A.rc + 1e-3 + 1e-5 * (info[0] + info[4] + info[8]));
+        s_rpre2[w] = rpre * rpre;
+      }
       __syncwarp();
     }
     const int k = it - cl.itemoff[I];
@@ -182,10 +194,24 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
                             (hi_.y + (T)A.rc * s_inv[4] < T(0.499)) && (hi_.z + (T)A.rc * s_inv[8] < T(0.499));
     const T cx = ci.x * s_m[0], cy = ci.y * s_m[4], cz = ci.z * s_m[8];
 
-    // excluded partners of atom i as sorted slots (-1: none; -1 >> 5 never equals a cluster)
-    int xs_i[kMaxExcl];
+    // Excluded partners of atom i are sorted slots (-1: none), read per tile from two 16-byte
+    // loads. Only tiles whose cluster J lies in the warp's range of partner clusters
+    // [x_lo, x_hi] (warp-uniform) can hold an excluded pair; the others skip the check.
+    const int4 *xs_row = reinterpret_cast<const int4 *>(A.exslot + si * kMaxExcl);
+    int x_lo, x_hi;
+    {
+      const int4 a = xs_row[0], b = xs_row[1];
+      const int xs[kMaxExcl] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      int lo = 0x7fffffff, hi = -1;
 #pragma unroll
-    for (int x = 0; x < kMaxExcl; ++x) xs_i[x] = A.exslot[si * kMaxExcl + x];
+      for (int x = 0; x < kMaxExcl; ++x)
+        if (xs[x] >= 0) {
+          lo = min(lo, xs[x] >> 5);
+          hi = max(hi, xs[x] >> 5);
+        }
+      x_lo = __reduce_min_sync(kFull, lo);
+      x_hi = __reduce_max_sync(kFull, hi);
+    }
     bool all_shifted = true;  // warp-uniform: no tile of the item needs the per-pair minimum image
 
     // stage the tiles and build their cutoff masks (pass 1)
@@ -217,15 +243,32 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
         pj.y += sy;
         pj.z += sz;
       }
-      s_pos[w][t][lane] = pj;
-      s_lj[w][t][lane] = A.lj[sj];
-      if constexpr (MODE == 2) s_u[w][t][lane] = A.u[sj];
-      if (sizeof(T) == 4) {
-        s_nx[w][t][lane] = -(float)pj.x;
-        s_ny[w][t][lane] = -(float)pj.y;
-        s_nz[w][t][lane] = -(float)pj.z;
+      bool keep_j = cl.sidx[sj] >= 0;
+      if (shifted && J != I) {
+        const T ex_ = fmax(fabs(pj.x - cx) - hi_.x * s_m[0], T(0)), ey_ = fmax(fabs(pj.y - cy) - hi_.y * s_m[4], T(0)),
+                ez_ = fmax(fabs(pj.z - cz) - hi_.z * s_m[8], T(0));
+        keep_j = keep_j && (ex_ * ex_ + ey_ * ey_ + ez_ * ez_ <= s_rpre2[w]);
       }
-      const unsigned jvalid = __ballot_sync(kFull, cl.sidx[sj] >= 0);
+      const unsigned keep = __ballot_sync(kFull, keep_j);
+      const unsigned lt_mask = lanemask_lt();
+      const int nkeep = __popc(keep);
+      const int n4 = (nkeep + 3) >> 2;
+      if (keep_j) {
+        const int slot = __popc(keep & lt_mask);
+        s_pos[w][t][slot] = pj;
+        s_lj[w][t][slot] = A.lj[sj];
+        if constexpr (MODE == 2) s_u[w][t][slot] = A.u[sj];
+        if (sizeof(T) == 4) {
+          s_nx[w][t][slot] = -(float)pj.x;
+          s_ny[w][t][slot] = -(float)pj.y;
+          s_nz[w][t][slot] = -(float)pj.z;
+        }
+      }
+      if (sizeof(T) == 4 && lane >= nkeep && lane < 4 * n4) {
+        s_nx[w][t][lane] = 1e18f;
+        s_ny[w][t][lane] = 1e18f;
+        s_nz[w][t][lane] = 1e18f;
+      }
       __syncwarp();
       unsigned mask = 0u;
       if (sizeof(T) == 4 && shifted) {
@@ -236,8 +279,9 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
         const float2 px = make_float2((float)pi.x, (float)pi.x), py = make_float2((float)pi.y, (float)pi.y),
                      pz = make_float2((float)pi.z, (float)pi.z);
         const float2 nrc2 = make_float2(-rc2_up, -rc2_up);
-#pragma unroll 2
+#pragma unroll
         for (int s = 0; s < kWarp; s += 4) {
+          if (s >= 4 * n4) break;
           const float4 nx = *reinterpret_cast<const float4 *>(&s_nx[w][t][s]);
           const float4 ny = *reinterpret_cast<const float4 *>(&s_ny[w][t][s]);
           const float4 nz = *reinterpret_cast<const float4 *>(&s_nz[w][t][s]);
@@ -257,10 +301,10 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
           mask = __funnelshift_l(__float_as_uint(d2.x), mask, 1);
           mask = __funnelshift_l(__float_as_uint(d2.y), mask, 1);
         }
-        mask = __brev(mask);
+        mask = n4 > 0 ? __brev(mask) >> (kWarp - 4 * n4) : 0u;
       } else {
-#pragma unroll 8
-        for (int s = 0; s < kWarp; ++s) {
+#pragma unroll 4
+        for (int s = 0; s < nkeep; ++s) {
           const V q = s_pos[w][t][s];
           T dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
           if (!shifted) pair_min_image(ortho, dx, dy, dz, s_m, s_inv);
@@ -268,14 +312,18 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMi
           mask |= (r2 <= rc2) ? (1u << s) : 0u;
         }
       }
-      mask &= jvalid;
-      if (J == I) mask &= ~(1u << lane);
+      if (nkeep < kWarp) mask &= (1u << nkeep) - 1u;
+      if (J == I) mask &= ~(1u << __popc(keep & lt_mask));
       if (!vi) mask = 0u;
       unsigned emask = 0u;
-      if (mask) {
+      if (J >= x_lo && J <= x_hi && mask) {
+        const int4 a = xs_row[0], b = xs_row[1];
+        const int xs[kMaxExcl] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-        for (int x = 0; x < kMaxExcl; ++x)
-          if ((xs_i[x] >> 5) == J) emask |= 1u << (xs_i[x] & 31);
+        for (int x = 0; x < kMaxExcl; ++x) {
+          const int o = xs[x] & 31;
+          if ((xs[x] >> 5) == J && ((keep >> o) & 1u)) emask |= 1u << __popc(keep & ((1u << o) - 1u));
+        }
       }
       s_mask[w][t][lane] = mask & ~emask;
       s_xmask[w][t][lane] = mask & emask;
