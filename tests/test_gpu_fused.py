@@ -122,9 +122,10 @@ def test_host_entry_point_matches_device(ref216):
 
 
 def test_host_entry_point_page_locked_buffers(ref216):
-    """Page-locked coords/forces take the one-graph path (copies inside the graph): results equal
-    the device path on consecutive calls with new coordinates, on a second pair of buffers, and
-    when the box is not page-locked."""
+    """Page-locked coords/forces take the one-graph path (a 648-atom box: kernels read the
+    coordinates and write the forces in host memory, no copies): results equal the device
+    path on consecutive calls with new coordinates, on a second pair of buffers, and when the
+    box is not page-locked."""
     from torchff_b200.system import FixedChargeSystem
 
     wb, _ = ref216
@@ -139,6 +140,26 @@ def test_host_entry_point_page_locked_buffers(ref216):
         hx.copy_(torch.from_numpy(x))
         e = sysm.evaluate_host(hx, box, hf)
         dev = sysm.evaluate(t(x, torch.float32), t(wb.box, torch.float32))
+        assert e == dev["energy"].item()
+        assert np.array_equal(hf.numpy().astype(np.float32), dev["forces"].cpu().numpy())
+
+
+def test_host_entry_point_page_locked_buffers_large():
+    """Above 1 MiB of coordinates (15,000 waters) the one-graph path copies inside the graph;
+    results equal the device path."""
+    from torchff_b200.system import FixedChargeSystem
+    from torchff_b200.water import serving_water_box
+
+    wb = serving_water_box(15000, seed=3)
+    assert 3 * wb.natoms * 8 > 1 << 20
+    sysm = FixedChargeSystem.from_water_box(wb, dtype=torch.float32)
+    hx = torch.from_numpy(np.ascontiguousarray(wb.coords, dtype=np.float64)).pin_memory()
+    hf = torch.empty((wb.natoms, 3), dtype=torch.float64).pin_memory()
+    for step in range(2):
+        if step:
+            hx.add_(0.001)
+        e = sysm.evaluate_host(hx, np.ascontiguousarray(wb.box), hf)
+        dev = sysm.evaluate(hx.to("cuda", torch.float32), t(wb.box, torch.float32))
         assert e == dev["energy"].item()
         assert np.array_equal(hf.numpy().astype(np.float32), dev["forces"].cpu().numpy())
 
