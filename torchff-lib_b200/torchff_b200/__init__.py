@@ -4,7 +4,8 @@ Importing the package loads libtffb200.so and registers the reference operator s
 under ``torch.ops.torchff``. Module classes keep the reference names and signatures:
 NeighborList, Nonbonded, Coulomb, Vdw, MultipolarInteraction (rank 0), PME (rank 0), PBC,
 HarmonicBond, HarmonicAngle, Angles; FixedChargeSystem / FixedChargeNonbonded evaluate the
-whole model (nonbonded, plus harmonic bonds and angles of flexible water) in one call.
+whole model (nonbonded, plus harmonic bonds and angles of flexible water) in one call;
+TorchSimModel serves torch-sim states of one or many systems.
 """
 from . import _lib  # noqa: F401  (fails loudly when the CUDA library is missing)
 from . import ops  # noqa: F401
@@ -21,6 +22,7 @@ from .pbc import PBC, applyPBC
 from .pme import PME
 from .serving import BatchEvaluator, Server, SystemSpec, autotune_atoms_per_cell
 from .system import FixedChargeNonbonded, FixedChargeSystem
+from .torchsim import Topology, TorchSimModel
 from .vdw import Vdw, compute_lennard_jones_energy
 
 __all__ = [
@@ -32,4 +34,5 @@ __all__ = [
     "compute_angles", "compute_harmonic_angle_energy", "HarmonicBond", "compute_harmonic_bond_energy",
     "build_cluster_pairs", "build_neighbor_list_cluster_pairs", "decode_cluster_pairs",
     "compute_nonbonded_energy_from_cluster_pairs", "compute_nonbonded_forces_from_cluster_pairs",
+    "Topology", "TorchSimModel",
 ]
