@@ -102,6 +102,32 @@ def test_fp64_water3000(ref3000):
     assert rel_max(out["forces"], -ref["grad_coords"]) < 1e-8
 
 
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_triclinic_box(dtype):
+    """A sheared 216-water box (rows a = (L,0,0), b = (0.15,L,0), c = (0.1,0.12,L) nm, every
+    perpendicular width above 2 rc): the fused system against the oracle, which takes the
+    minimum image through fractional coordinates as torchff/pbc.py:59-62 does."""
+    from torchff_b200.system import FixedChargeSystem
+    from torchff_b200.water import water_box_216
+
+    wb = water_box_216()
+    L = wb.box[0, 0]
+    box = np.array([[L, 0.0, 0.0], [0.15, L, 0.0], [0.1, 0.12, L]])
+    ref = O.fixed_charge_energy(wb.coords, box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
+                                wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
+                                138.935456)
+    sysm = FixedChargeSystem(wb.charges, wb.sigma, wb.epsilon, wb.coulomb_exclusions, wb.cutoff, wb.alpha,
+                             wb.grid, dtype=dtype)
+    out = sysm.evaluate(t(wb.coords, dtype), t(box, dtype))
+    assert sysm.status() == 0
+    if dtype == torch.float64:
+        assert rel(out["energy"].item(), ref["total"]) < 1e-10
+        assert rel_max(out["forces"], -ref["grad_coords"]) < 1e-8
+    else:
+        assert _mixed_energy_err(out["energy"].item(), ref) < 1e-6
+        assert rel_rms(out["forces"], -ref["grad_coords"]) < 1e-5
+
+
 def test_host_entry_point_matches_device(ref216):
     from torchff_b200.system import FixedChargeSystem
 

@@ -89,6 +89,20 @@ def test_overflow_reports_count(algorithm):
     assert all(tuple(p) in s for p in got.tolist())
 
 
+def test_cell_list_count_equals_nsquared_at_one_million_atoms():
+    """The reference's large-system check (tests/test_nblist.py:230-250): 1,000,000 uniformly
+    random atoms at 100 atoms/nm^3 (L = 21.54 nm), FP64, rc = 0.8 nm; the cell list finds as
+    many pairs as the all-pairs search. Both report the full count when the pair buffer
+    overflows, so a small buffer serves."""
+    n = 1_000_000
+    box_len = (n / 100.0) ** (1.0 / 3.0)
+    rng = np.random.default_rng(5)
+    x = torch.tensor(rng.uniform(0.0, box_len, (n, 3)), device="cuda")
+    box = torch.tensor(np.diag([box_len] * 3), device="cuda")
+    counts = [int(_op(a)(x, box, 0.8, 1024, None, None, False)[1].item()) for a in ALGOS]
+    assert counts[0] == counts[1] > 100 * n
+
+
 @pytest.mark.parametrize("algorithm", ALGOS)
 def test_out_variant_and_trim(algorithm):
     from torchff_b200 import nblist as nb
