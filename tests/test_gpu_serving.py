@@ -134,3 +134,48 @@ def test_server_request_alone_equals_request_in_a_mix(mixed_boxes):
     assert rel(eb, ea) < 1e-9
     assert rel_max(fb, fa) < 1e-6
     srv.close()
+
+
+def test_faulty_requests_are_refused_and_the_rest_served():
+    """Failures injected on the host. Requests beyond the per-request limits (16,386 atoms,
+    a 97^3 PME grid; a lane always has room for one request within them), one with an
+    exclusion index outside its own system and one with more than 8 excluded partners for an
+    atom are refused at submission (invalid argument); a wait on a held
+    server gives up after its timeout and the request still completes once the hold is
+    lifted. The requests around the refused ones are served with the results a batch of
+    their own gives."""
+    from dataclasses import replace
+
+    from torchff_b200.serving import Server, SystemSpec
+    from torchff_b200.water import serving_water_box
+
+    wbs, specs = _boxes([150, 300, 500], seed0=300)
+    srv = Server(RC, wbs[0].alpha, torch.float32, lanes=2, max_systems_per_batch=8, hbm_budget_bytes=64 << 20)
+    huge = SystemSpec.from_water_box(serving_water_box(5462, seed=1))
+    assert huge.natoms > 16384
+    with pytest.raises(RuntimeError, match="invalid"):
+        srv.submit(huge)
+    with pytest.raises(RuntimeError, match="invalid"):
+        srv.submit(replace(specs[0], pme_grid=97))
+    n0 = specs[0].natoms
+    with pytest.raises(RuntimeError, match="invalid"):
+        srv.submit(replace(specs[0], excl_pairs=np.array([[0, n0]], dtype=np.int64)))
+    with pytest.raises(RuntimeError, match="invalid"):
+        srv.submit(replace(specs[0], excl_pairs=np.array([[0, j] for j in range(1, 10)], dtype=np.int64)))
+    srv.hold(True)
+    held = srv.submit(specs[1])
+    with pytest.raises(RuntimeError, match="timeout"):
+        held.wait(timeout=0.2)
+    srv.hold(False)
+    reqs = [held] + [srv.submit(s) for s in specs]
+    srv.drain(timeout=60)
+    assert srv.stats()["systems_done"] == 4
+    ev = _evaluator(torch.float32, wbs)
+    for r, s in zip(reqs, [specs[1]] + specs):
+        e, f = ev.evaluate([s])
+        torch.cuda.synchronize()
+        en, fn = r.wait(timeout=10)
+        assert rel(en, e.item()) < 1e-9
+        assert rel_max(fn, f[0]) < 1e-6
+        r.release()
+    srv.close()

@@ -406,6 +406,7 @@ int tff_batch_destroy(tff_batch b) {
 int tff_batch_eval(tff_batch b, int nsys, const int64_t *natoms, const int *pme_grid, const void *coords,
                    const void *boxes, const void *charges, const void *sigma, const void *epsilon, const int *excl,
                    double *energies, void *forces, tff_stream_t stream) {
+  TFF_NVTX("tff_batch_eval");
   TFF_ARG(b != nullptr, "batch is NULL");
   TFF_ARG(nsys >= 1 && nsys <= b->desc.max_systems, "nsys %d outside [1, %d]", nsys, b->desc.max_systems);
   TFF_ARG(natoms && pme_grid && coords && boxes && charges && sigma && epsilon && excl && energies && forces,

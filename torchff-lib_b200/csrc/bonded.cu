@@ -105,6 +105,7 @@ size_t tff_bonded_workspace_bytes(int dtype, int64_t natoms, int64_t nterms) {
 int tff_harmonic_bond(int dtype, int64_t natoms, const void *coords, int64_t nbonds, const int64_t *bonds,
                       const void *b0, const void *k, void *energy, void *grad_coords, void *grad_b0, void *grad_k,
                       void *workspace, size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_harmonic_bond");
   BondedCall c{dtype, false, natoms, nbonds, coords, bonds, b0, k, energy, grad_coords, grad_b0, grad_k, 1.0,
                false, workspace, workspace_bytes};
   return run_bonded_any(c, (cudaStream_t)stream);
@@ -113,6 +114,7 @@ int tff_harmonic_bond(int dtype, int64_t natoms, const void *coords, int64_t nbo
 int tff_harmonic_bond_forces(int dtype, int64_t natoms, const void *coords, int64_t nbonds, const int64_t *bonds,
                              const void *b0, const void *k, void *forces, void *workspace, size_t workspace_bytes,
                              tff_stream_t stream) {
+  TFF_NVTX("tff_harmonic_bond_forces");
   TFF_ARG(forces != nullptr || natoms == 0, "forces is NULL");
   BondedCall c{dtype, false, natoms, nbonds, coords, bonds, b0, k, nullptr, forces, nullptr, nullptr, -1.0,
                true, workspace, workspace_bytes};
@@ -122,6 +124,7 @@ int tff_harmonic_bond_forces(int dtype, int64_t natoms, const void *coords, int6
 int tff_harmonic_angle(int dtype, int64_t natoms, const void *coords, int64_t nangles, const int64_t *angles,
                        const void *theta0, const void *k, void *energy, void *grad_coords, void *grad_theta0,
                        void *grad_k, void *workspace, size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_harmonic_angle");
   BondedCall c{dtype, true, natoms, nangles, coords, angles, theta0, k, energy, grad_coords, grad_theta0, grad_k,
                1.0, false, workspace, workspace_bytes};
   return run_bonded_any(c, (cudaStream_t)stream);
@@ -130,6 +133,7 @@ int tff_harmonic_angle(int dtype, int64_t natoms, const void *coords, int64_t na
 int tff_harmonic_angle_forces(int dtype, int64_t natoms, const void *coords, int64_t nangles, const int64_t *angles,
                               const void *theta0, const void *k, void *forces, void *workspace,
                               size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_harmonic_angle_forces");
   TFF_ARG(forces != nullptr || natoms == 0, "forces is NULL");
   BondedCall c{dtype, true, natoms, nangles, coords, angles, theta0, k, nullptr, forces, nullptr, nullptr, -1.0,
                true, workspace, workspace_bytes};
@@ -139,6 +143,7 @@ int tff_harmonic_angle_forces(int dtype, int64_t natoms, const void *coords, int
 int tff_angles(int dtype, int64_t natoms, const void *coords, int64_t nangles, const int64_t *angles, void *theta,
                const void *grad_theta, void *grad_coords, void *workspace, size_t workspace_bytes,
                tff_stream_t stream) {
+  TFF_NVTX("tff_angles");
   TFF_ARG(dtype == TFF_F32 || dtype == TFF_F64, "dtype must be TFF_F32 or TFF_F64");
   TFF_ARG(natoms >= 0 && nangles >= 0, "negative sizes");
   TFF_ARG(nangles == 0 || (coords != nullptr && angles != nullptr), "coords / angles is NULL");

@@ -629,6 +629,7 @@ int tff_cluster_pairs_build(int dtype, int64_t natoms, const void *coords, const
                             int32_t *tiles, uint32_t *tile_masks, int64_t tiles_cap, int32_t *entry_cluster,
                             int32_t *entry_atoms, int64_t entries_cap, int64_t *counts, int max_cluster_neighbors,
                             void *workspace, size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_cluster_pairs_build");
   TFF_ARG(dtype == TFF_F32 || dtype == TFF_F64, "dtype must be TFF_F32 or TFF_F64");
   TFF_ARG(box != nullptr, "build_cluster_pairs requires a periodic box");
   TFF_ARG(natoms >= 0 && tiles_cap >= 0 && entries_cap >= 0, "negative sizes");
@@ -655,6 +656,7 @@ int tff_cluster_pairs_decode(int dtype, int64_t natoms, const void *coords, cons
                              const uint32_t *tile_masks, const int32_t *entry_cluster, const int32_t *entry_atoms,
                              int64_t nentries, int32_t *pairs, int64_t max_npairs, int32_t *npairs,
                              tff_stream_t stream) {
+  TFF_NVTX("tff_cluster_pairs_decode");
   TFF_ARG(dtype == TFF_F32 || dtype == TFF_F64, "dtype must be TFF_F32 or TFF_F64");
   TFF_ARG(box != nullptr, "decode_cluster_pairs requires a periodic box");
   TFF_ARG(coords != nullptr || natoms == 0, "coords is NULL");
@@ -699,6 +701,7 @@ int tff_nonbonded_cluster_pairs(int dtype, int64_t natoms, const void *coords, c
                                 const int32_t *entry_atoms, int64_t nentries, void *energy, void *energy_coulomb,
                                 void *grad_coords, void *grad_sigma, void *grad_epsilon, void *grad_charges,
                                 void *workspace, size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_nonbonded_cluster_pairs");
   TFF_ARG(dtype == TFF_F32 || dtype == TFF_F64, "dtype must be TFF_F32 or TFF_F64");
   TFF_ARG(box != nullptr, "the cluster-pair nonbonded term requires a periodic box");
   TFF_ARG(natoms == 0 || (coords && sigma && epsilon && charges), "coords / sigma / epsilon / charges is NULL");
@@ -727,6 +730,7 @@ int tff_nonbonded_forces_cluster_pairs(int dtype, int64_t natoms, const void *co
                                        const uint32_t *tile_masks, const int32_t *entry_cluster,
                                        const int32_t *entry_atoms, int64_t nentries, void *forces, void *workspace,
                                        size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_nonbonded_forces_cluster_pairs");
   TFF_ARG(dtype == TFF_F32 || dtype == TFF_F64, "dtype must be TFF_F32 or TFF_F64");
   TFF_ARG(box != nullptr, "the cluster-pair nonbonded term requires a periodic box");
   TFF_ARG(natoms == 0 || (coords && sigma && epsilon && charges && forces), "an input array is NULL");

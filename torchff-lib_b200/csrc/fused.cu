@@ -538,6 +538,7 @@ int tff_system_set_parameters(tff_system sys, const void *charges, const void *s
 
 int tff_system_eval(tff_system sys, const void *coords, const void *box, double *energy, void *forces,
                     void *grad_charges, double *energy_terms, tff_stream_t stream) {
+  TFF_NVTX("tff_system_eval");
   TFF_ARG(sys != nullptr, "system is NULL");
   TFF_ARG(box != nullptr, "box is NULL");
   TFF_ARG(sys->desc.natoms == 0 || coords != nullptr, "coords is NULL");
@@ -642,6 +643,7 @@ extern "C" {
 
 int tff_system_eval_host(tff_system sys, const double *coords, const double *box, double *energy, double *forces,
                          tff_stream_t stream) {
+  TFF_NVTX("tff_system_eval_host");
   TFF_ARG(sys != nullptr, "system is NULL");
   TFF_ARG(box != nullptr && energy != nullptr, "box/energy is NULL");
   const int64_t n = sys->desc.natoms;
@@ -720,6 +722,7 @@ int tff_timer_elapsed_ms(tff_timer timer, int from, int to, float *ms) {
 
 int tff_system_eval_timed(tff_system sys, const void *coords, const void *box, double *energy, void *forces,
                           tff_timer timer, tff_stream_t stream) {
+  TFF_NVTX("tff_system_eval_timed");
   TFF_ARG(sys != nullptr && timer != nullptr, "system/timer is NULL");
   TFF_ARG(box != nullptr, "box is NULL");
   TFF_ARG(sys->desc.natoms == 0 || coords != nullptr, "coords is NULL");
@@ -733,6 +736,7 @@ int tff_system_eval_timed(tff_system sys, const void *coords, const void *box, d
 
 int tff_system_eval_grads(tff_system sys, const void *coords, const void *box, double *energy, void *forces,
                           void *grad_charges, void *grad_sigma, void *grad_epsilon, tff_stream_t stream) {
+  TFF_NVTX("tff_system_eval_grads");
   TFF_ARG(sys != nullptr && box != nullptr, "system/box is NULL");
   TFF_ARG(sys->desc.natoms == 0 || coords != nullptr, "coords is NULL");
   cudaStream_t s = (cudaStream_t)stream;
@@ -746,6 +750,7 @@ int tff_system_eval_grads(tff_system sys, const void *coords, const void *box, d
 
 int tff_system_hvp(tff_system sys, const void *coords, const void *box, const void *direction, void *hvp_coords,
                    void *hvp_charges, void *hvp_sigma, void *hvp_epsilon, tff_stream_t stream) {
+  TFF_NVTX("tff_system_hvp");
   TFF_ARG(sys != nullptr && box != nullptr, "system/box is NULL");
   TFF_ARG(sys->desc.natoms == 0 || (coords != nullptr && direction != nullptr), "coords/direction is NULL");
   cudaStream_t s = (cudaStream_t)stream;

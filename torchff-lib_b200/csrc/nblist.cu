@@ -284,6 +284,7 @@ extern "C" {
 int tff_nblist_nsquared(int dtype, int64_t natoms, const void *coords, const void *box, double cutoff,
                         const int64_t *excl_row_ptr, const int64_t *excl_col, int include_self, int64_t *pairs,
                         int64_t max_npairs, int32_t *npairs, tff_stream_t stream) {
+  TFF_NVTX("tff_nblist_nsquared");
   TFF_ARG(dtype == TFF_F32 || dtype == TFF_F64, "dtype must be TFF_F32 or TFF_F64");
   TFF_ARG(natoms >= 0 && max_npairs >= 0, "negative sizes");
   TFF_ARG(npairs != nullptr, "npairs is NULL");
@@ -308,6 +309,7 @@ int tff_nblist_cell_list(int dtype, int64_t natoms, const void *coords, const vo
                          const int64_t *excl_row_ptr, const int64_t *excl_col, int include_self, int64_t *pairs,
                          int64_t max_npairs, int32_t *npairs, int max_cluster_neighbors, void *workspace,
                          size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_nblist_cell_list");
   TFF_ARG(dtype == TFF_F32 || dtype == TFF_F64, "dtype must be TFF_F32 or TFF_F64");
   TFF_ARG(box != nullptr, "Cell-list neighbor list requires a periodic box");
   TFF_ARG(natoms >= 0 && max_npairs >= 0, "negative sizes");

@@ -428,6 +428,7 @@ int tff_nonbonded_atom_pairs(int dtype, int64_t natoms, const void *coords, int6
                              double cutoff, int do_shift, void *energy, void *grad_coords,
                              void *grad_sigma, void *grad_epsilon, void *grad_charges,
                              void *workspace, size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_nonbonded_atom_pairs");
   PairCall c{};
   c.dtype = dtype;
   c.cm = do_shift ? C_SHIFT : C_PLAIN;
@@ -446,6 +447,7 @@ int tff_nonbonded_forces_atom_pairs(int dtype, int64_t natoms, const void *coord
                                     const void *sigma, const void *epsilon, const void *charges,
                                     double coul_constant, double cutoff, void *forces,
                                     void *workspace, size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_nonbonded_forces_atom_pairs");
   TFF_ARG(forces != nullptr || natoms == 0, "forces is NULL");
   PairCall c{};
   c.dtype = dtype;
@@ -463,6 +465,7 @@ int tff_coulomb_atom_pairs(int dtype, int64_t natoms, const void *coords, int64_
                            double coul_constant, double cutoff, int do_shift, void *energy,
                            void *grad_coords, void *grad_charges, void *workspace,
                            size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_coulomb_atom_pairs");
   PairCall c{};
   c.dtype = dtype;
   c.cm = do_shift ? C_SHIFT : C_PLAIN;
@@ -482,6 +485,7 @@ int tff_lennard_jones_atom_pairs(int dtype, int64_t natoms, const void *coords, 
                                  int64_t ntypes, void *energy, void *grad_coords,
                                  void *grad_sigma, void *grad_epsilon, void *workspace,
                                  size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_lennard_jones_atom_pairs");
   PairCall c{};
   c.dtype = dtype;
   c.cm = C_NONE;
@@ -502,6 +506,7 @@ int tff_ewald_real_atom_pairs(int dtype, int64_t natoms, const void *coords, con
                               double ewald_alpha, double prefactor, void *energy,
                               void *grad_coords, void *grad_charges, void *workspace,
                               size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_ewald_real_atom_pairs");
   PairCall c{};
   c.dtype = dtype;
   const bool ewald = ewald_alpha >= 0.0;

@@ -80,6 +80,7 @@ size_t tff_pme_workspace_bytes(tff_pme_plan plan, int64_t natoms) {
 int tff_pme_long_range(tff_pme_plan plan, int64_t natoms, const void *coords, const void *box, const void *charges,
                        double alpha, const void *xmoduli, const void *ymoduli, const void *zmoduli, void *energy,
                        void *phi, void *grad_coords, void *workspace, size_t workspace_bytes, tff_stream_t stream) {
+  TFF_NVTX("tff_pme_long_range");
   TFF_ARG(plan != nullptr, "plan is NULL");
   TFF_ARG(natoms >= 0, "negative natoms");
   TFF_ARG(box != nullptr, "PME requires a periodic box");

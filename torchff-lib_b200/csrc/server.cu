@@ -205,6 +205,7 @@ void pack_requests(const Lane &l, size_t ts, const std::vector<int64_t> &off, in
 }
 
 int launch_lane(tff_server s, Lane &l) {
+  TFF_NVTX("tff_server_batch");
   const size_t ts = s->ts;
   const int nsys = (int)l.reqs.size();
   l.natoms.resize(nsys);

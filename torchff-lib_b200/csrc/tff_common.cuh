@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "tffb200.h"
 
 namespace tff {
@@ -30,6 +32,16 @@ int sm_count();
   } while (0)
 
 #define TFF_LAUNCHED() TFF_CUDA(cudaGetLastError())
+
+// Host-side NVTX range around the enqueue work of one entry point (shown by Nsight Systems
+// beside the kernels it launched; free when no tool is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
+#define TFF_NVTX(name) ::tff::NvtxRange tff_nvtx_range_(name)
 
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;
