@@ -89,6 +89,26 @@ def test_overflow_reports_count(algorithm):
     assert all(tuple(p) in s for p in got.tolist())
 
 
+@pytest.mark.parametrize("algorithm", ALGOS)
+def test_module_grows_a_short_capacity(algorithm):
+    """NeighborList with max_npairs far below the pair count: by default it builds again with
+    the exact count and returns the full list (the reference truncates); with
+    grow_on_overflow=False it warns and returns the first max_npairs pairs."""
+    from torchff_b200.nblist import NeighborList
+    from torchff_b200.water import water_box_216
+
+    wb = water_box_216()
+    excl = torch.tensor(wb.nblist_exclusions)
+    want = O.canonical_pairs(_oracle_pairs(wb.coords, wb.box, wb.cutoff, wb.nblist_exclusions, wb.natoms, False,
+                                           torch.float64))
+    got = NeighborList(wb.natoms, exclusions=excl, algorithm=algorithm).cuda()(t(wb.coords), t(wb.box), wb.cutoff, 1000)
+    assert np.array_equal(canon(got), want)
+    short = NeighborList(wb.natoms, exclusions=excl, algorithm=algorithm, grow_on_overflow=False).cuda()
+    with pytest.warns(UserWarning, match="truncated"):
+        cut = short(t(wb.coords), t(wb.box), wb.cutoff, 1000)
+    assert cut.shape[0] == 1000
+
+
 def test_cell_list_count_equals_nsquared_at_one_million_atoms():
     """The reference's large-system check (tests/test_nblist.py:230-250): 1,000,000 uniformly
     random atoms at 100 atoms/nm^3 (L = 21.54 nm), FP64, rc = 0.8 nm; the cell list finds as

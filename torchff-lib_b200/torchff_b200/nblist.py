@@ -6,6 +6,11 @@ tiled all-pairs test, ``"cell_list"`` bins atoms on a Hilbert-ordered cell grid,
 them in 32-atom clusters and tests cluster pairs with 32x32 warp tiles.
 ``use_customized_ops`` is accepted for signature compatibility; there is no second
 implementation behind it.
+
+When ``max_npairs`` is too small, the reference's ``NeighborList`` returns a truncated list
+(torchff/nblist.py:162-178). Both kernels here count every pair past the capacity, so
+``NeighborList`` builds once more with the exact size and returns the full list; pass
+``grow_on_overflow=False`` to keep the truncation (with a warning).
 """
 from __future__ import annotations
 
@@ -37,10 +42,15 @@ def convert_pairs_coo_to_csr(pairs_coo: torch.Tensor, num_atoms: Optional[int] =
     return row_ptr, cols
 
 
+# npairs of the cell list when a cluster's neighbour-cluster list overflowed (pair count unknown)
+CLUSTER_LIST_OVERFLOW = 2 ** 31 - 1
+
+
 class NeighborList(nn.Module):
     def __init__(self, natoms: int, exclusions: torch.Tensor | None = None, include_self: bool = False,
-                 use_customized_ops: bool = True, algorithm: str = "nsquared"):
+                 use_customized_ops: bool = True, algorithm: str = "nsquared", *, grow_on_overflow: bool = True):
         super().__init__()
+        self.grow_on_overflow = grow_on_overflow
         if algorithm not in ("nsquared", "cell_list"):
             raise ValueError(f"algorithm must be 'nsquared' or 'cell_list', got '{algorithm}'")
         self.natoms = natoms
@@ -80,7 +90,13 @@ class NeighborList(nn.Module):
         if padding:
             return pairs, npairs
         found = int(npairs.item())
+        if found == CLUSTER_LIST_OVERFLOW and self.algorithm == "cell_list":
+            raise RuntimeError("cell list: a cluster has more neighbour clusters than the list holds "
+                               "(cutoff too large for the cell grid); use algorithm='nsquared'")
         if found > pairs.shape[0]:
+            if self.grow_on_overflow:
+                # the count is exact: one more build with room for every pair
+                return self.forward(coords, box, cutoff, found, padding)
             warnings.warn(f"neighbour list truncated: found {found} pairs, capacity {pairs.shape[0]}",
                           stacklevel=2)
         return pairs[:found]
