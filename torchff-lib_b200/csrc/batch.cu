@@ -112,6 +112,7 @@ struct tff_batch_s {
   cudaEvent_t table_ev = nullptr;  // the table upload of the previous evaluation
   cudaStream_t pme_stream = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  cudaEvent_t sorted_ev = nullptr;  // batch sort done (the PME gather visits its atom order)
   std::vector<BatchSys> host_sys;
   int device = 0;
 };
@@ -127,6 +128,7 @@ void free_batch(tff_batch b) {
   if (b->pme_stream) cudaStreamDestroy(b->pme_stream);
   if (b->fork_ev) cudaEventDestroy(b->fork_ev);
   if (b->join_ev) cudaEventDestroy(b->join_ev);
+  if (b->sorted_ev) cudaEventDestroy(b->sorted_ev);
   delete b;
 }
 
@@ -272,15 +274,18 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
                                                         e_pme);
   TFF_LAUNCHED();
   if ((st = run_dft<T>(dsys, nsys, kmax, false, real, cplx, ps)) != TFF_OK) return st;
-  batch_gather_kernel<T><<<pgrid, kPmeBlock, 0, ps>>>(dsys, x, q, boxes, real, b->desc.ewald_alpha, pme_phi, pme_grad,
-                                                      partials, tickets, e_pme);
-  TFF_LAUNCHED();
-  TFF_CUDA(cudaEventRecord(b->join_ev, ps));
 
   // --- real space on the caller stream
   batch_sort_kernel<T><<<(int)std::min<int64_t>(nsys, 2 * sms), kBatchSortThreads, kBatchSortSmem, s>>>(x, q, boxes,
                                                                                                      nsys, cd);
   TFF_LAUNCHED();
+  // the PME gather follows the sort's atom order
+  TFF_CUDA(cudaEventRecord(b->sorted_ev, s));
+  TFF_CUDA(cudaStreamWaitEvent(ps, b->sorted_ev, 0));
+  batch_gather_kernel<T><<<pgrid, kPmeBlock, 0, ps>>>(dsys, x, q, cd.sidx, boxes, real, b->desc.ewald_alpha, pme_phi,
+                                                      pme_grad, partials, tickets, e_pme);
+  TFF_LAUNCHED();
+  TFF_CUDA(cudaEventRecord(b->join_ev, ps));
   cluster_bounds_kernel<T><<<(int)std::max<int64_t>(1, std::min<int64_t>(nsup, 2 * sms)), kWarp * kSuper, 0, s>>>(cd);
   TFF_LAUNCHED();
   const int nb_cl = (int)std::max<int64_t>(1, std::min<int64_t>((ncl + 3) / 4, sms * 16));
@@ -369,6 +374,7 @@ int tff_batch_create(const tff_batch_desc *desc, tff_batch *out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->pme_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->sorted_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) {
     // B-spline moduli of every grid size the batch accepts
     std::vector<double> mod;

@@ -26,6 +26,7 @@ struct tff_system_s {
   tff_pme_plan pme = nullptr;
   cudaStream_t pme_stream = nullptr;  // PME runs here, forked from / joined to the caller stream
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  cudaEvent_t built_ev = nullptr;  // cluster build done (the PME gather visits its atom order)
   void *cl_ws = nullptr;
   void *pme_ws = nullptr;
   void *acc = nullptr;         // gx (npad*3), gq, gsigma, ga (npad each): zeroed per evaluation
@@ -102,33 +103,28 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
   const int sms = sm_count();
   S *energies = reinterpret_cast<S *>(sys->scratch);  // real-space energy accumulators, zeroed by the build
 
-  // --- PME on the side stream: needs only the caller's coordinates and the charges
+  // --- PME on the side stream: the grid phase needs only the caller's coordinates and the
+  // charges; the gather (enqueued after the cluster build below) visits the atoms in the
+  // build's cluster order, so that neighbouring threads read neighbouring grid points
   const bool use_pme = sys->pme && n > 0;
   const double *e_pme = nullptr;
+  cudaStream_t ps = sys->pme_stream;
+  char *pw = static_cast<char *>(sys->pme_ws);
+  T *phi_grid = nullptr;
   if (use_pme) {
     TFF_CUDA(cudaEventRecord(sys->fork_ev, s));
-    TFF_CUDA(cudaStreamWaitEvent(sys->pme_stream, sys->fork_ev, 0));
-    cudaStream_t ps = sys->pme_stream;
+    TFF_CUDA(cudaStreamWaitEvent(ps, sys->fork_ev, 0));
     const int K = sys->desc.pme_grid;
     const T *xm = static_cast<const T *>(sys->moduli);
     const T *ym = xm + K;
     const T *zm = ym + K;
-    char *pw = static_cast<char *>(sys->pme_ws);
     PlainAtoms<T> atoms{x, static_cast<const T *>(sys->q), n};
-    T *phi_grid = nullptr;
     // bonded terms ride on the PME stream (a few microseconds, off the real-space chain)
     if (sys->has_bonded() && (st = launch_bonded<T>(sys, x, ps)) != TFF_OK) return st;
     st = pme_grid_phase<T>(sys->pme->impl, sys->pl, pw, atoms, n, box, sys->desc.ewald_alpha, xm, ym, zm, ps,
                            &phi_grid);
     if (st != TFF_OK) return st;
     if ((st = mark(3, ps)) != TFF_OK) return st;
-    PlainGatherOut<T> out{static_cast<T *>(sys->pme_phi), static_cast<T *>(sys->pme_grad)};
-    st = pme_gather_phase<T>(sys->pme->impl, sys->pl, pw, atoms, n, box, sys->desc.ewald_alpha, phi_grid, out, 1.0,
-                             (T *)nullptr, ps);
-    if (st != TFF_OK) return st;
-    if ((st = mark(4, ps)) != TFF_OK) return st;
-    TFF_CUDA(cudaEventRecord(sys->join_ev, ps));
-    e_pme = reinterpret_cast<const double *>(pw + sys->pl.energies);
   }
 
   if (!use_pme && sys->has_bonded() && n > 0 && (st = launch_bonded<T>(sys, x, s)) != TFF_OK) return st;
@@ -142,6 +138,18 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
                          /*half=*/0, s, sys->scratch, 8 * sizeof(double), pdl);
   if (st != TFF_OK) return st;
   if ((st = mark(1, s)) != TFF_OK) return st;
+  if (use_pme) {
+    TFF_CUDA(cudaEventRecord(sys->built_ev, s));
+    TFF_CUDA(cudaStreamWaitEvent(ps, sys->built_ev, 0));
+    IndexedAtoms<T> ia{x, static_cast<const T *>(sys->q), cd.sidx, sys->cl.npad};
+    IndexedGatherOut<T> out{static_cast<T *>(sys->pme_phi), static_cast<T *>(sys->pme_grad), cd.sidx};
+    st = pme_gather_phase<T>(sys->pme->impl, sys->pl, pw, ia, sys->cl.npad, box, sys->desc.ewald_alpha, phi_grid,
+                             out, 1.0, (T *)nullptr, ps);
+    if (st != TFF_OK) return st;
+    if ((st = mark(4, ps)) != TFF_OK) return st;
+    TFF_CUDA(cudaEventRecord(sys->join_ev, ps));
+    e_pme = reinterpret_cast<const double *>(pw + sys->pl.energies);
+  }
   S *gx = static_cast<S *>(sys->acc);
   S *gq = gx + 3 * sys->cl.npad;
   auto *lj = static_cast<typename V2<T>::type *>(sys->lj);
@@ -340,6 +348,7 @@ void free_system(tff_system sys) {
   if (sys->pme_stream) cudaStreamDestroy(sys->pme_stream);
   if (sys->fork_ev) cudaEventDestroy(sys->fork_ev);
   if (sys->join_ev) cudaEventDestroy(sys->join_ev);
+  if (sys->built_ev) cudaEventDestroy(sys->built_ev);
   if (sys->host_graph) cudaGraphExecDestroy(sys->host_graph);
   if (sys->pinned_graph) cudaGraphExecDestroy(sys->pinned_graph);
   if (sys->pinned_io) cudaFreeHost(sys->pinned_io);
@@ -424,6 +433,7 @@ int tff_system_create(const tff_system_desc *desc, const double *charges, const 
   cudaError_t e = cudaStreamCreateWithFlags(&sys->pme_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sys->fork_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sys->join_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sys->built_ev, cudaEventDisableTiming);
   auto upload = [&](void *dst, const double *src, int64_t cnt) {
     if (cnt == 0 || e != cudaSuccess) return;
     if (ts == 8) {

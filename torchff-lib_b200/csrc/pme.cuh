@@ -92,6 +92,26 @@ struct SortedAtoms {
   }
 };
 
+// Atoms in the cluster (Hilbert) order of a cluster build: slot t is caller atom sidx[t]
+// (-1: padding). Coordinates and charges come from the caller arrays, so every atom's
+// numbers are those of PlainAtoms; only the visiting order changes, and neighbouring
+// threads then touch neighbouring grid points.
+template <class T>
+struct IndexedAtoms {
+  const T *x;
+  const T *q;
+  const int *sidx;
+  int64_t n;  // slots
+  __device__ __forceinline__ bool get(int64_t t, double &rx, double &ry, double &rz, T &qi) const {
+    if (t >= n) return false;
+    const int64_t a = sidx[t];
+    if (a < 0) return false;
+    rx = x[3 * a]; ry = x[3 * a + 1]; rz = x[3 * a + 2];
+    qi = q[a];
+    return true;
+  }
+};
+
 // Spread: a group of kLanesPerAtom lanes per atom; lane g of the group takes the stencil
 // rows r = g, g + kLanesPerAtom, ... of the 36 (x, y) rows, 6 z points each. Loops run at
 // warp granularity so that every lane of a warp takes the same trip count. `bid` and
@@ -210,6 +230,23 @@ struct PlainGatherOut {
       grad[3 * t] = (T)gx;
       grad[3 * t + 1] = (T)gy;
       grad[3 * t + 2] = (T)gz;
+    }
+  }
+};
+
+// Gather output for IndexedAtoms: slot t's values go to caller atom sidx[t].
+template <class T>
+struct IndexedGatherOut {
+  T *phi;   // dE/dq (N), nullable
+  T *grad;  // dE/dx (N,3), nullable
+  const int *sidx;
+  __device__ __forceinline__ void put(int64_t t, double phi_t, double gx, double gy, double gz) const {
+    const int64_t a = sidx[t];
+    if (phi) phi[a] = (T)phi_t;
+    if (grad) {
+      grad[3 * a] = (T)gx;
+      grad[3 * a + 1] = (T)gy;
+      grad[3 * a + 2] = (T)gz;
     }
   }
 };
@@ -584,19 +621,24 @@ __global__ void __launch_bounds__(kPmeBlock) batch_convolve_kernel(const BatchSy
 }
 
 template <class T>
+// The atoms of a system are visited in the cluster order of the batch's sort (sidx: sorted
+// slot -> batch atom index, -1 for padding), so that neighbouring threads read neighbouring
+// grid points; each atom's numbers are those of the caller-order visit.
 __global__ void __launch_bounds__(kPmeBlock) batch_gather_kernel(const BatchSys *sys, const T *x, const T *q,
-                                                                 const T *boxes, const T *Phi, double alpha, T *phi,
-                                                                 T *grad, double *partials, unsigned *tickets,
-                                                                 double *energies) {
+                                                                 const int *sidx, const T *boxes, const T *Phi,
+                                                                 double alpha, T *phi, T *grad, double *partials,
+                                                                 unsigned *tickets, double *energies) {
   const int sy = blockIdx.y;
   const BatchSys &b = sys[sy];
   if (blockIdx.x >= (unsigned)b.pme_blocks) return;
   __shared__ PmeShared sh;
   if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
   __syncthreads();
-  PlainAtoms<T> atoms{x + 3 * b.atom_off, q + b.atom_off, b.natoms};
-  PlainGatherOut<T> out{phi + b.atom_off, grad + 3 * b.atom_off};
-  const double e = gather_atoms<T>(atoms, b.natoms, sh, b.K, Phi + b.grid_off, alpha, out, blockIdx.x, b.pme_blocks);
+  const int *slots = sidx + b.cl_off * kWarp;
+  const int64_t nslots = b.ncl * kWarp;
+  IndexedAtoms<T> atoms{x, q, slots, nslots};
+  IndexedGatherOut<T> out{phi, grad, slots};
+  const double e = gather_atoms<T>(atoms, nslots, sh, b.K, Phi + b.grid_off, alpha, out, blockIdx.x, b.pme_blocks);
   grid_sum_n<kPmeBlock>(e, partials + (int64_t)kBatchPmeMaxBlocks * sy, tickets + 2 * sy + 1, energies + 2 * sy + 1,
                         false, blockIdx.x, b.pme_blocks);
 }
