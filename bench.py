@@ -158,9 +158,9 @@ def measured_peaks() -> dict:
         return {}
 
 
-def ncu_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch from the committed ncu summary, if one exists."""
-    path = os.path.join(REPO, "profiles", "ncu_traffic.txt")
+def ncu_traffic(kernel: str, workload: str, name: str = "ncu_traffic.txt"):
+    """A per-launch figure (DRAM bytes by default) from a committed ncu summary, if one exists."""
+    path = os.path.join(REPO, "profiles", name)
     try:
         with open(path) as f:
             for ln in f:
@@ -570,6 +570,10 @@ def run_ours(args):
                                f"{tile_mean_ms * 1e3:.2f} us (CUDA events in the graph)",
                 "peak_source": f"FP32 nominal 148 SM x 128 lanes x 2 flop x {sm_max:.0f} MHz (sm_max_mhz of "
                                "MEASURED_PEAKS.json; no measured FP32 peak exists)",
+                "issue_active": ncu_traffic("tile_kernel", args.workload, "ncu_issue.txt"),
+                "issue_note": "the tile kernel is bound by instruction issue (mask building, bit walk, "
+                              "pair math), not by the FP32 pipe: fraction of issue slots used, from ncu "
+                              "(profiles/ncu_issue.txt)",
             },
             "clocks": clk,
         }
