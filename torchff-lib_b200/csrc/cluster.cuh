@@ -29,6 +29,8 @@ constexpr int kItemTiles = 4;
 // Consecutive clusters per super-cluster: the neighbour search screens a super-cluster's
 // union box first and tests its members only when that box is within the cutoff.
 constexpr int kSuper = 32;
+// Histograms up to this many keys are scanned by the last block of the key kernel.
+constexpr int64_t kFusedScanMaxKeys = 8192;
 
 template <class T> struct V4;
 template <> struct V4<float> { using type = float4; };
@@ -242,35 +244,10 @@ __global__ void box_info_kernel(const T *box, double *info, unsigned long long *
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nz2; k += stride) z2[k] = 0ull;
 }
 
-template <class T>
-__global__ void cell_keys_kernel(const T *x, int64_t n, ClusterData<T> d) {
-  pdl_enter();
-  const double *inv = d.boxinfo + 9;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    double rx = x[3 * i], ry = x[3 * i + 1], rz = x[3 * i + 2];
-    double f[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double v = rx * inv[c] + ry * inv[3 + c] + rz * inv[6 + c];
-      v -= floor(v);
-      if (v >= 1.0) v = 0.0;  // guards rounding of tiny negatives
-      f[c] = v;
-    }
-    unsigned cell[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) cell[c] = min((unsigned)(f[c] * d.nc), (unsigned)(d.nc - 1));
-    const unsigned key = hilbert_key(cell[0], cell[1], cell[2], d.bits);
-    d.keys[i] = key;
-    atomicAdd(&d.hist[key], 1u);
-  }
-}
-
 // Exclusive scan of hist[0..nkeys) in place; hist[nkeys] = total. One block of 1024
 // threads; thread t owns a contiguous segment, so the work is two sweeps of the segment
 // plus one block-wide scan of the segment sums.
-static __global__ void scan_keys_kernel(unsigned *hist, int64_t nkeys) {
-  pdl_enter();
+__device__ __forceinline__ void scan_keys_body(unsigned *hist, int64_t nkeys) {
   __shared__ unsigned s_warp[32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   // segments of whole 4-key chunks read as uint4 (hist is 16-byte aligned), several loads in
@@ -327,6 +304,48 @@ static __global__ void scan_keys_kernel(unsigned *hist, int64_t nkeys) {
     run += v;
   }
   if (threadIdx.x == blockDim.x - 1) hist[nkeys] = run;
+}
+
+template <class T>
+// With scan_nkeys > 0 (small systems) the last block to finish also scans the histogram
+// (status[4] is its block ticket, zeroed per build), which saves the scan launch.
+__global__ void cell_keys_kernel(const T *x, int64_t n, ClusterData<T> d, int64_t scan_nkeys) {
+  pdl_enter();
+  const double *inv = d.boxinfo + 9;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double rx = x[3 * i], ry = x[3 * i + 1], rz = x[3 * i + 2];
+    double f[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double v = rx * inv[c] + ry * inv[3 + c] + rz * inv[6 + c];
+      v -= floor(v);
+      if (v >= 1.0) v = 0.0;  // guards rounding of tiny negatives
+      f[c] = v;
+    }
+    unsigned cell[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) cell[c] = min((unsigned)(f[c] * d.nc), (unsigned)(d.nc - 1));
+    const unsigned key = hilbert_key(cell[0], cell[1], cell[2], d.bits);
+    d.keys[i] = key;
+    atomicAdd(&d.hist[key], 1u);
+  }
+  if (scan_nkeys <= 0) return;
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&d.status[4], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  scan_keys_body(d.hist, scan_nkeys);
+}
+
+static __global__ void scan_keys_kernel(unsigned *hist, int64_t nkeys) {
+  pdl_enter();
+  scan_keys_body(hist, nkeys);
 }
 
 template <class T>
@@ -814,8 +833,12 @@ int build_clusters(const ClusterLayout &L, const ClusterData<T> &d, void *ws, co
   if (st != TFF_OK) return st;
   if (L.natoms == 0) return TFF_OK;
   const int nb_atoms = (int)std::max<int64_t>(1, std::min<int64_t>((L.natoms + 255) / 256, sms * 8));
-  if ((st = launch_k(pdl, cell_keys_kernel<T>, nb_atoms, 256, 0, s, x, L.natoms, d)) != TFF_OK) return st;
-  if ((st = launch_k(pdl, scan_keys_kernel, 1, 1024, 0, s, d.hist, L.nkeys)) != TFF_OK) return st;
+  // up to kFusedScanMaxKeys keys the last block of the key kernel scans the histogram
+  const bool fused_scan = L.nkeys <= kFusedScanMaxKeys;
+  if ((st = launch_k(pdl, cell_keys_kernel<T>, nb_atoms, 256, 0, s, x, L.natoms, d,
+                     (int64_t)(fused_scan ? L.nkeys : 0))) != TFF_OK)
+    return st;
+  if (!fused_scan && (st = launch_k(pdl, scan_keys_kernel, 1, 1024, 0, s, d.hist, L.nkeys)) != TFF_OK) return st;
   if ((st = launch_k(pdl, scatter_atoms_kernel<T>, nb_atoms, 256, 0, s, L.natoms, d)) != TFF_OK) return st;
   const int nb_keys = (int)std::max<int64_t>(1, std::min<int64_t>((L.nkeys + 3) / 4, sms * 32));
   if ((st = launch_k(pdl, sort_buckets_kernel<T>, nb_keys, 128, 0, s, x, q, L.nkeys, d)) != TFF_OK) return st;
