@@ -405,7 +405,8 @@ int tff_system_create(const tff_system_desc *desc, const double *charges, const 
   const size_t ts = desc->dtype == TFF_F64 ? 8 : 4;
 #define TFF_ALLOC(ptr, bytes)                                              \
   do {                                                                     \
-    cudaError_t _e = cudaMalloc((void **)&(ptr), (bytes) ? (bytes) : 256); \
+    const size_t _b = (bytes);                                             \
+    cudaError_t _e = cudaMalloc((void **)&(ptr), _b ? _b : 256);           \
     if (_e != cudaSuccess) {                                               \
       free_system(sys);                                                    \
       return cuda_fail(_e, "cudaMalloc", __FILE__, __LINE__);              \
