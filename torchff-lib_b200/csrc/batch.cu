@@ -315,7 +315,7 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
     const int64_t max_items = ncl * ((L.cap + kItemTiles - 1) / kItemTiles);
     constexpr int NW = TileCfg<T>::NW;
     const int nbt = (int)std::max<int64_t>(1, std::min<int64_t>((max_items + NW - 1) / NW, (int64_t)sms * 48 / NW));
-    tile_kernel<T><<<nbt, NW * kWarp, 0, s>>>(A);
+    tile_kernel<T, 0, kTileMinBlocksBatch><<<nbt, NW * kWarp, 0, s>>>(A);
     TFF_LAUNCHED();
   }
   TFF_CUDA(cudaStreamWaitEvent(s, b->join_ev, 0));

@@ -121,11 +121,13 @@ __device__ __forceinline__ void pair_min_image(bool ortho, T &dx, T &dy, T &dz, 
 }
 
 // Resident 4-warp blocks per SM the register allocation of the energy kernel must allow
-// (6 blocks = 24 warps: at most 80 registers per thread).
+// (6 blocks = 24 warps: at most 80 registers per thread). The batched evaluation, whose
+// many small systems leave more work items in flight, runs best at 7 (at most 73).
 constexpr int kTileMinBlocks = 6;
+constexpr int kTileMinBlocksBatch = 7;
 
-template <class T, int MODE = 0>
-__global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? kTileMinBlocks : 1)
+template <class T, int MODE = 0, int MIN_BLOCKS = kTileMinBlocks>
+__global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? MIN_BLOCKS : 1)
     tile_kernel(TileArgs<T> A) {
   pdl_enter();
   using V = typename V4<T>::type;
