@@ -128,6 +128,48 @@ def test_triclinic_box(dtype):
         assert rel_rms(out["forces"], -ref["grad_coords"]) < 1e-5
 
 
+@pytest.mark.parametrize("n_waters", [1, 2, 11])
+def test_tiny_systems(n_waters):
+    """One, two and eleven waters in a 2.0 nm box (rc 0.9 nm, K = 20): one partial cluster,
+    and for one water no pair beyond its own excluded ones (exclusion correction and PME
+    only). FP64 against the oracle (energy 1e-10, forces 1e-8 of the largest). In mixed
+    precision the net force on a lone water is what remains of two terms of about
+    k |q_O q_H| / r_OH^2 = 5,300 kJ/mol/nm (the reciprocal sum and the exclusion correction)
+    that cancel to a few kJ/mol/nm, so its error is bounded against that term: every force
+    component within 1e-6 of it; the energy within the usual mixed tolerance."""
+    from torchff_b200.system import FixedChargeSystem
+    from torchff_b200.water import make_water_box
+
+    wb = make_water_box(n_waters, 2.0, 3, 0.9, 20, seed=5)
+    ref = _oracle(wb)
+    for dtype in (torch.float64, torch.float32):
+        sysm = FixedChargeSystem.from_water_box(wb, dtype=dtype)
+        out = sysm.evaluate(t(wb.coords, dtype), t(wb.box, dtype))
+        assert sysm.status() == 0
+        if dtype == torch.float64:
+            assert rel(out["energy"].item(), ref["total"]) < 1e-10
+            assert rel_max(out["forces"], -ref["grad_coords"]) < 1e-8
+        else:
+            assert _mixed_energy_err(out["energy"].item(), ref) < 1e-6
+            term = 138.935456 * 0.834 * 0.417 / 0.09572 ** 2
+            err = np.abs(out["forces"].double().cpu().numpy() + ref["grad_coords"]).max()
+            assert err < 1e-6 * term, err
+
+
+def test_empty_system():
+    """A system of no atoms evaluates to zero energy and an empty force array."""
+    from torchff_b200.system import FixedChargeSystem
+    from torchff_b200.water import water_box_216
+
+    wb = water_box_216()
+    for dtype in (torch.float64, torch.float32):
+        sysm = FixedChargeSystem(np.zeros(0), np.zeros(0), np.zeros(0), None, wb.cutoff, wb.alpha, wb.grid,
+                                 dtype=dtype)
+        out = sysm.evaluate(torch.zeros((0, 3), dtype=dtype, device="cuda"), t(wb.box, dtype))
+        assert out["energy"].item() == 0.0 and out["forces"].shape == (0, 3)
+        assert sysm.status() == 0
+
+
 def test_host_entry_point_matches_device(ref216):
     from torchff_b200.system import FixedChargeSystem
 
