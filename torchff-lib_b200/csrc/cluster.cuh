@@ -24,7 +24,9 @@ namespace tff {
 
 // Neighbour clusters per tile-kernel work item (a work item is one cluster I and every
 // (ncount/kItemTiles)-th cluster of its list). 4 gives a 9000-atom box ~5,600 warps of work,
-// enough to fill 148 SMs; 8 measured 3 % slower there and equal at 300,000 atoms.
+// enough to fill 148 SMs; 8 measured 3 % slower there and equal at 300,000 atoms; 3 and 2
+// measured 3 % and 6 % slower at 9000 atoms and 4 % and 10 % slower at 300,000 atoms (more
+// items hold the SMs longer against the PME kernels of the other stream).
 constexpr int kItemTiles = 4;
 // Consecutive clusters per super-cluster: the neighbour search screens a super-cluster's
 // union box first and tests its members only when that box is within the cutoff.
