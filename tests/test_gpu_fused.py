@@ -92,6 +92,30 @@ def test_mixed_water3000_accuracy_and_determinism(ref3000):
     assert sysm.status() == 0
 
 
+def test_mixed_shuffled_atoms():
+    """A 216-water box with its atoms in a random order (molecules no longer contiguous, the
+    exclusions renumbered): repeated mixed-precision evaluations are bit-identical and match
+    the oracle, forces mapped back to the original order, within the mixed tolerances."""
+    from torchff_b200.system import FixedChargeSystem
+    from torchff_b200.water import water_box_216
+
+    wb = water_box_216()
+    perm = np.random.default_rng(3).permutation(wb.natoms)
+    inv = np.argsort(perm)
+    coords = wb.coords[perm]
+    excl = inv[wb.coulomb_exclusions]
+    ref = _oracle(wb)
+    sysm = FixedChargeSystem(wb.charges[perm], wb.sigma[perm], wb.epsilon[perm], excl, wb.cutoff, wb.alpha, wb.grid,
+                             dtype=torch.float32)
+    x, b = t(coords, torch.float32), t(wb.box, torch.float32)
+    outs = [sysm.evaluate(x, b) for _ in range(3)]
+    for o in outs[1:]:
+        assert torch.equal(o["energy"], outs[0]["energy"]) and torch.equal(o["forces"], outs[0]["forces"])
+    assert _mixed_energy_err(outs[0]["energy"].item(), ref) < 1e-6
+    assert rel_rms(outs[0]["forces"][torch.as_tensor(inv, device="cuda")], -ref["grad_coords"]) < 1e-5
+    assert sysm.status() == 0
+
+
 def test_fp64_water3000(ref3000):
     from torchff_b200.system import FixedChargeSystem
 
