@@ -27,6 +27,54 @@ def test_library_exports_every_declared_symbol():
     assert set(declared) == set(_lib.EXPORTED)
 
 
+def _header_prototypes():
+    """name -> (return class, [argument classes]) for every prototype in the header; classes
+    are int / int64 / double / size_t / ptr (pointers, handles and the stream type)."""
+    src = open(os.path.join(REPO, "include", "tffb200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"//[^\n]*", "", src)
+    src = re.sub(r"^\s*#[^\n]*", "", src, flags=re.M)
+    handles = set(re.findall(r"typedef\s+struct\s+\w+\s*\*\s*(\w+)\s*;", src))
+
+    def cls(decl):
+        decl = decl.strip()
+        if "*" in decl:
+            return "ptr"
+        words = decl.replace("const ", "").split()
+        base = words[0]
+        if base in handles:
+            return "ptr"
+        return {"int": "int", "int64_t": "int64", "double": "double", "size_t": "size_t"}[base]
+
+    out = {}
+    for ret, name, params in re.findall(r"(\b[A-Za-z_][\w\s\*]*?)\b(tff_\w+)\s*\(([^;{]*?)\)\s*;", src):
+        args = [p for p in (q.strip() for q in params.split(",")) if p and p != "void"]
+        out[name] = (cls(ret + " x"), [cls(a) for a in args])
+    return out
+
+
+def test_ctypes_signatures_match_the_header():
+    """Every entry point's ctypes binding has the header's arity and argument types, so a
+    changed prototype cannot silently shift the arguments of a Python caller."""
+    import ctypes as C
+
+    from torchff_b200 import _lib
+
+    def cls(t):
+        if t is None:
+            return "void"
+        if t in (C.c_void_p, C.c_char_p) or (isinstance(t, type) and issubclass(t, C._Pointer)):
+            return "ptr"
+        return {C.c_int: "int", C.c_int64: "int64", C.c_double: "double", C.c_size_t: "size_t"}[t]
+
+    protos = _header_prototypes()
+    assert set(protos) == set(_lib._SIGS)
+    for name, (ret, args) in protos.items():
+        res, argtypes = _lib._SIGS[name]
+        assert cls(res) == ret, name
+        assert [cls(a) for a in argtypes] == args, name
+
+
 def test_pure_queries_need_no_gpu():
     from torchff_b200 import _lib
 
