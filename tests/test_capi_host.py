@@ -75,6 +75,20 @@ def test_ctypes_signatures_match_the_header():
         assert [cls(a) for a in argtypes] == args, name
 
 
+def test_integration_ctypes_stub_matches_the_header():
+    """The ctypes stub that the integration guide gives maintainers to paste declares the
+    header's argument types in the header's order."""
+    text = open(os.path.join(REPO, "INTEGRATION.md")).read()
+    stubs = re.findall(r"lib\.(tff_\w+)\.argtypes\s*=\s*\[(.*?)\]", text, flags=re.S)
+    assert stubs
+    kinds = {"c_int": "int", "c_int64": "int64", "c_double": "double", "c_size_t": "size_t", "c_void_p": "ptr",
+             "c_char_p": "ptr"}
+    protos = _header_prototypes()
+    for name, body in stubs:
+        args = [kinds[a.strip().split(".")[-1]] for a in body.split(",") if a.strip()]
+        assert args == protos[name][1], name
+
+
 def test_pure_queries_need_no_gpu():
     from torchff_b200 import _lib
 
