@@ -496,7 +496,8 @@ int tff_server_poll(tff_server server, int64_t ticket, int *done);
 /* Submission, batch start and completion times of a request on the server clock. */
 int tff_server_request_times(tff_server server, int64_t ticket, double *t_submit, double *t_start,
                              double *t_done);
-/* Forgets a finished request. */
+/* Forgets a finished request; refused (TFF_ERR_INVALID) while another thread is inside
+ * tff_server_wait on it. */
 int tff_server_release(tff_server server, int64_t ticket);
 /* Blocks until every submitted request is done. */
 int tff_server_drain(tff_server server, double timeout_s);

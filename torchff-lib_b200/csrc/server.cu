@@ -38,6 +38,7 @@ struct ServerReq {
   double t_submit = 0.0, t_start = 0.0, t_done = 0.0;
   int status = TFF_OK;
   bool done = false;
+  int waiters = 0;  // threads inside tff_server_wait on this request (release refuses while > 0)
 };
 
 struct Lane {
@@ -74,6 +75,7 @@ struct tff_server_s {
   std::thread worker;
   bool stop = false;
   bool hold = false;  // no new batch starts while set (requests keep queueing)
+  int waiting = 0;    // threads inside tff_server_wait / tff_server_drain (destroy waits for 0)
   int fatal = TFF_OK;
   std::chrono::steady_clock::time_point t0;
   tff_server_stats stats{};
@@ -343,6 +345,10 @@ void free_server(tff_server s) {
     }
     s->cv_work.notify_all();
     s->worker.join();
+    // every request is done now; let threads still inside a wait leave it before the
+    // mutex and the requests go away
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_done.wait(lk, [&] { return s->waiting == 0; });
   }
   for (Lane &l : s->lanes) free_lane(l);
   for (auto &kv : s->reqs) delete kv.second;  // every queued request is in the map too
@@ -501,9 +507,17 @@ int tff_server_wait(tff_server s, int64_t ticket, double timeout_s) {
   TFF_ARG(it != s->reqs.end(), "unknown ticket %lld", (long long)ticket);
   ServerReq *r = it->second;
   const auto pred = [&] { return r->done; };
-  if (timeout_s < 0) {
+  r->waiters += 1;  // keeps r alive: tff_server_release refuses a request that has waiters
+  s->waiting += 1;
+  bool finished = true;
+  if (timeout_s < 0)
     s->cv_done.wait(lk, pred);
-  } else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred)) {
+  else
+    finished = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred);
+  r->waiters -= 1;
+  s->waiting -= 1;
+  s->cv_done.notify_all();
+  if (!finished) {
     set_error("request %lld not finished within %.3f s", (long long)ticket, timeout_s);
     return TFF_ERR_TIMEOUT;
   }
@@ -537,6 +551,7 @@ int tff_server_release(tff_server s, int64_t ticket) {
   auto it = s->reqs.find(ticket);
   TFF_ARG(it != s->reqs.end(), "unknown ticket %lld", (long long)ticket);
   TFF_ARG(it->second->done, "request %lld is still in flight", (long long)ticket);
+  TFF_ARG(it->second->waiters == 0, "request %lld has a thread waiting on it", (long long)ticket);
   delete it->second;
   s->reqs.erase(it);
   return TFF_OK;
@@ -546,9 +561,15 @@ int tff_server_drain(tff_server s, double timeout_s) {
   TFF_ARG(s != nullptr, "server is NULL");
   std::unique_lock<std::mutex> lk(s->mu);
   const auto pred = [&] { return s->stats.systems_done >= s->stats.submitted || s->fatal != TFF_OK; };
-  if (timeout_s < 0) {
+  s->waiting += 1;
+  bool finished = true;
+  if (timeout_s < 0)
     s->cv_done.wait(lk, pred);
-  } else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred)) {
+  else
+    finished = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred);
+  s->waiting -= 1;
+  s->cv_done.notify_all();
+  if (!finished) {
     set_error("server not drained within %.3f s", timeout_s);
     return TFF_ERR_TIMEOUT;
   }
