@@ -172,6 +172,21 @@ def ncu_traffic(kernel: str, workload: str, name: str = "ncu_traffic.txt"):
     return None
 
 
+def throughput_fields(npairs: int, evals_per_s: float, tile_ms: float, tile_dram_bytes) -> dict:
+    """Pair throughput of the whole evaluation and the DRAM bandwidth the tile kernel draws.
+
+    npairs: in-cutoff pairs of the box (each pair once); evals_per_s: the line's value;
+    tile_ms: mean tile-kernel time per launch; tile_dram_bytes: dram__bytes_read.sum +
+    dram__bytes_write.sum of one tile-kernel launch from the committed ncu summary (None if
+    absent)."""
+    out = {"pairs_per_s": round(npairs * evals_per_s), "unit": "in-cutoff pairs per second, each pair once"}
+    if tile_dram_bytes is not None and tile_ms > 0:
+        out["tile_kernel_dram_gbs"] = round(tile_dram_bytes / (tile_ms * 1e-3) / 1e9, 2)
+        out["dram_note"] = ("DRAM bytes of one tile-kernel launch (ncu) / its mean CUDA-event time: positions "
+                            "are re-read from L2, so the kernel draws little HBM bandwidth")
+    return out
+
+
 def cpu_baseline_sample(wb, evals: int = 2) -> dict:
     from oracle import oracle as O
 
@@ -577,6 +592,7 @@ def run_ours(args):
             },
             "clocks": clk,
         }
+        result["throughput"] = throughput_fields(npairs, value, tile_mean_ms, ncu_traffic("tile_kernel", args.workload))
         if fm is not None:
             result["force_matching"] = fm
         if world == 1 and not args.no_fp64 and dtype == torch.float32:

@@ -89,6 +89,22 @@ def test_integration_ctypes_stub_matches_the_header():
         assert args == protos[name][1], name
 
 
+def test_bench_throughput_fields():
+    """The pair-throughput / DRAM-bandwidth object of the bench line: pairs x evals/s, and the
+    tile kernel's ncu DRAM bytes over its event time (left out when no ncu figure exists)."""
+    import importlib.util
+    import json
+
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(REPO, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    f = bench.throughput_fields(1891879, 9646.67, 0.0669, 1035904.0)
+    assert f["pairs_per_s"] == round(1891879 * 9646.67)
+    assert abs(f["tile_kernel_dram_gbs"] - 1035904.0 / 66.9e-6 / 1e9) < 0.01
+    assert "tile_kernel_dram_gbs" not in bench.throughput_fields(10, 1.0, 1.0, None)
+    json.dumps(f)
+
+
 def test_pure_queries_need_no_gpu():
     from torchff_b200 import _lib
 
