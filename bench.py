@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOAD_TEXT), default="water3000")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=200)
@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 timing of the water3000 line")
     ap.add_argument("--serving-requests", type=int, default=4096)
     ap.add_argument("--no-force-matching", action="store_true", help="skip the force-matching section")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference CUDA ops timing (reference_gpu) of the line")
     return ap.parse_args()
 
 
@@ -109,16 +111,19 @@ class ClockSampler:
             out, _ = self.proc.communicate()
         self.lines = [ln for ln in out.splitlines() if ln.strip()]
 
-    def summary(self) -> dict:
+    def summary(self, window=None) -> dict:
+        """Median SM clock and the throttle reasons seen in [begin(), end()], or in
+        window = (first, last) datetimes when given."""
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        lo, hi = window if window is not None else (self.t_begin, self.t_end)
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 10:
                 continue
             try:
                 ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f")
-                if self.t_begin is not None and not (self.t_begin <= ts <= self.t_end):
+                if lo is not None and not (lo <= ts <= hi):
                     continue
                 sm.append(float(f[2]))
                 smax = float(f[3])
@@ -158,18 +163,44 @@ def measured_peaks() -> dict:
         return {}
 
 
+PROFILED_SOURCES = ("tile.cuh", "cluster.cuh", "tff_common.cuh", "fused.cu")
+
+
+def kernel_source_hash() -> str:
+    """sha256 (16 hex digits) of the real-space kernel sources, as the ncu summaries record
+    it: a summary captured from other sources is stale for this build."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for name in PROFILED_SOURCES:
+        with open(os.path.join(REPO, "torchff-lib_b200", "csrc", name), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
 def ncu_traffic(kernel: str, workload: str, name: str = "ncu_traffic.txt"):
-    """A per-launch figure (DRAM bytes by default) from a committed ncu summary, if one exists."""
+    """A per-launch figure (DRAM bytes by default) from a committed ncu summary, with the
+    date and source hash it records; the value is None when the summary is absent or was
+    captured from other kernel sources than this build's."""
     path = os.path.join(REPO, "profiles", name)
+    meta = {"file": f"profiles/{name}", "value": None}
     try:
         with open(path) as f:
             for ln in f:
                 p = ln.split()
-                if len(p) >= 3 and p[0] == kernel and p[1] == workload:
-                    return float(p[2])
+                if ln.startswith("# source-hash"):
+                    meta["source_hash"] = p[2]
+                elif ln.startswith("# captured"):
+                    meta["captured"] = p[2]
+                elif len(p) >= 3 and p[0] == kernel and p[1] == workload:
+                    meta["value"] = float(p[2])
     except OSError:
-        pass
-    return None
+        return meta
+    current = kernel_source_hash()
+    if meta.get("source_hash") != current:
+        meta["stale"] = f"captured from sources {meta.get('source_hash')}, this build is {current}"
+        meta["value"] = None
+    return meta
 
 
 def throughput_fields(npairs: int, evals_per_s: float, tile_ms: float, tile_dram_bytes) -> dict:
@@ -187,18 +218,34 @@ def throughput_fields(npairs: int, evals_per_s: float, tile_ms: float, tile_dram
     return out
 
 
-def cpu_baseline_sample(wb, evals: int = 2) -> dict:
+def cpu_baseline_sample(wb, evals: int = 2) -> tuple[dict, dict]:
+    """The numpy oracle timed on one host core over `evals` evaluations of the box; also
+    returns the oracle's FP64 result, which the accuracy figures of the line use."""
     from oracle import oracle as O
 
     t0 = time.perf_counter()
     for _ in range(evals):
-        O.fixed_charge_energy(wb.coords, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
-                              wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
-                              138.935456)
+        ref = O.fixed_charge_energy(wb.coords, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
+                                    wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
+                                    138.935456)
     dt = time.perf_counter() - t0
-    return {"value": evals / dt, "unit": "evals/s", "cores": 1, "kind": "port",
-            "sample": f"{evals} full evaluations of the same box by the numpy oracle (O(N^2) neighbour list, "
-                      f"pair terms, PME with analytic forces), one thread"}
+    return ({"value": evals / dt, "unit": "evals/s", "cores": 1, "kind": "port",
+             "sample": f"{evals} full evaluations of the same box by the numpy oracle (O(N^2) neighbour list, "
+                       f"pair terms, PME with analytic forces), one thread"}, ref)
+
+
+def accuracy_vs_oracle(energy: float, forces, ref: dict) -> dict:
+    """Energy and force error of one result against the FP64 oracle on the same box."""
+    import numpy as np
+
+    f0 = -ref["grad_coords"]
+    f = np.asarray(forces, dtype=np.float64)
+    return {"energy_kj_mol": energy, "oracle_energy_kj_mol": float(ref["total"]),
+            "energy_abs_err": float(f"{abs(energy - ref['total']):.3g}"),
+            "energy_rel_err": float(f"{abs(energy - ref['total']) / abs(ref['total']):.3g}"),
+            "force_rms_rel_err": float(f"{np.sqrt(np.mean((f - f0) ** 2)) / np.sqrt(np.mean(f0 ** 2)):.3g}"),
+            "force_max_abs_err": float(f"{np.max(np.abs(f - f0)):.3g}"),
+            "reference": "numpy FP64 oracle (restatement of the reference pure-torch path) on the same box"}
 
 
 def time_graph_evals(wb, dtype, device, steps: int, warmup: int) -> dict:
@@ -237,7 +284,8 @@ def time_graph_evals(wb, dtype, device, steps: int, warmup: int) -> dict:
         total += start.elapsed_time(end)
     del graph
     return {"value": round(steps / (total / 1e3), 2), "unit": "evals/s", "ms_per_step": round(total / steps, 5),
-            "steps": steps, "warmup": warmup}
+            "steps": steps, "warmup": warmup,
+            "_result": (float(energy.item()), forces.double().cpu().numpy())}
 
 
 def run_force_matching(device, dtype, rank: int, world: int, frames: int = 16, steps: int = 10,
@@ -434,7 +482,12 @@ def run_ours(args):
     import torchff_b200  # noqa: F401
     from torchff_b200.system import FixedChargeSystem, StageTimer
 
+    # one sampler for the whole run: the timed steps are the window [begin(), end()]
+    clocks = ClockSampler(local)
+    clocks.start()
+    run_t0 = datetime.datetime.now()
     if args.workload == "serving":
+        clocks.stop()
         run_serving_line(args, device, rank, world)
         return
     dtype = torch.float32 if args.precision == "mixed" else torch.float64
@@ -472,8 +525,6 @@ def run_ours(args):
         graph.replay()
     torch.cuda.synchronize(device)
 
-    clocks = ClockSampler(local)
-    clocks.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(device)
@@ -490,7 +541,6 @@ def run_ours(args):
     clocks.end()
     if world > 1:
         dist.barrier()
-    clocks.stop()
     # stage breakdown (and the tile-kernel time of the roofline) from the graph with events
     n_stage = min(args.steps, 200)
     tile_ms, stage_acc = [], {k: 0.0 for k in StageTimer.STAGES}
@@ -545,7 +595,8 @@ def run_ours(args):
         flops = 60.0 * npairs                                   # algorithmic flops per launch
         achieved = flops / (tile_mean_ms * 1e-3) / 1e12
         stages = {k: round(v / n_stage * 1e3, 3) for k, v in stage_acc.items()}
-        clk = clocks.summary()
+        traffic = ncu_traffic("tile_kernel", args.workload)
+        issue = ncu_traffic("tile_kernel", args.workload, "ncu_issue.txt")
         result = {
             "metric": METRIC if args.workload == "water3000" else f"{args.workload} PME energy+force evals/s",
             "value": round(value, 2),
@@ -580,32 +631,57 @@ def run_ours(args):
                 "peak": round(fp32_peak, 2),
                 "unit": "TFLOP/s",
                 "frac": round(achieved / fp32_peak, 5),
-                "traffic": ncu_traffic("tile_kernel", args.workload),
+                "traffic": traffic["value"],
+                "traffic_source": traffic,
                 "algorithmic": f"60 flop x {npairs} in-cutoff pairs per launch / mean tile-kernel time "
                                f"{tile_mean_ms * 1e3:.2f} us (CUDA events in the graph)",
                 "peak_source": f"FP32 nominal 148 SM x 128 lanes x 2 flop x {sm_max:.0f} MHz (sm_max_mhz of "
                                "MEASURED_PEAKS.json; no measured FP32 peak exists)",
-                "issue_active": ncu_traffic("tile_kernel", args.workload, "ncu_issue.txt"),
+                "issue_active": issue["value"],
+                "issue_source": issue,
                 "issue_note": "the tile kernel is bound by instruction issue (mask building, bit walk, "
                               "pair math), not by the FP32 pipe: fraction of issue slots used, from ncu "
                               "(profiles/ncu_issue.txt)",
             },
-            "clocks": clk,
         }
-        result["throughput"] = throughput_fields(npairs, value, tile_mean_ms, ncu_traffic("tile_kernel", args.workload))
+        result["throughput"] = throughput_fields(npairs, value, tile_mean_ms, traffic["value"])
         if fm is not None:
             result["force_matching"] = fm
+        fp64_result = None
         if world == 1 and not args.no_fp64 and dtype == torch.float32:
             result["fp64"] = time_graph_evals(wb, torch.float64, device, min(args.steps, 500), args.warmup)
+            fp64_result = result["fp64"].pop("_result")
         if world == 1 and not args.no_serving:
             result["serving"] = run_serving(device, args.serving_requests)
+        oracle_ref = None
         if world == 1 and not args.no_cpu_baseline:
             if args.workload == "water100k":
                 result["cpu_baseline"] = {"value": None, "unit": "evals/s", "cores": 0, "kind": "port",
                                           "sample": "not run: the reference CPU path's O(N^2) pair search over "
                                                     "300,000 atoms (4.5e10 pairs) is infeasible"}
             else:
-                result["cpu_baseline"] = cpu_baseline_sample(wb)
+                result["cpu_baseline"], oracle_ref = cpu_baseline_sample(wb)
+        if oracle_ref is not None:
+            # the result the timed graph produced (last replay) and the FP64 one, against the oracle
+            result["accuracy"] = {("mixed" if dtype == torch.float32 else "fp64"):
+                                  accuracy_vs_oracle(float(energy.item()), forces.double().cpu().numpy(), oracle_ref)}
+            if fp64_result is not None:
+                result["accuracy"]["fp64"] = accuracy_vs_oracle(fp64_result[0], fp64_result[1], oracle_ref)
+        if world == 1 and not args.no_reference_gpu and args.workload in ("water3000", "water216"):
+            rg = reference_gpu_leg(args)
+            result["reference_gpu"] = rg
+            if "value" in rg and rg.get("value"):
+                result["speedup_vs_reference_fp64_cuda"] = {
+                    "device": round(value / rg["value"], 2), "e2e": round(e2e_value / rg["value"], 2),
+                    "formula": "this line's value (and e2e value) / reference_gpu.value (the reference's FP64 CUDA "
+                               "ops on the same box and GPU, CUDA graph, L2 flushed)"}
+        clocks.stop()
+        result["clocks"] = clocks.summary()
+        result["clocks_whole_run"] = dict(clocks.summary((run_t0, datetime.datetime.now())), note=(
+            "nvidia-smi samples over the whole run of this line (timed steps, stage timing, e2e, force matching, "
+            "FP64, serving, reference GPU): the timed steps alone can be shorter than one 50 ms sample"))
+    else:
+        clocks.stop()
     del graph
     if world > 1:
         dist.barrier()
@@ -650,8 +726,181 @@ def run_serving_line(args, device, rank, world):
 
 
 # ---------------------------------------------------------------------------------------
-# reference arm: the CPU restatement of the reference's pure-torch path
+# reference arm: the reference's own pure-torch path on the host cores
 # ---------------------------------------------------------------------------------------
+
+REF_EXTENSIONS = ("torchff_bond", "torchff_angle", "torchff_nblist", "torchff_nb", "torchff_coulomb", "torchff_vdw",
+                  "torchff_multipoles", "torchff_pme", "torchff_torsion", "torchff_dispersion", "torchff_slater",
+                  "torchff_ewald", "torchff_amoeba", "torchff_cmm")
+
+
+def import_reference_cpu():
+    """The reference package (THGLab/torchff-lib, installed without its CUDA extensions into
+    baseline/_ref) imported for its pure-torch path. Its modules import their compiled
+    extension modules by name; the pure-torch path never calls them, so empty modules stand
+    in. torchff/pme_ref.py:8 switches the default device to CUDA at import time; it is set
+    back to the CPU afterwards. Returns None when the install is absent."""
+    import types
+
+    root = os.path.join(REPO, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(root, "torchff")):
+        return None
+    import torch
+
+    for name in REF_EXTENSIONS:
+        sys.modules.setdefault(name, types.ModuleType(name))
+    sys.path.insert(0, root)
+    import torchff  # noqa: F401
+    from torchff.multipoles import MultipolarInteraction
+    from torchff.nblist import NeighborList
+    from torchff.pme import PME
+    from torchff.vdw import Vdw
+
+    torch.set_default_device("cpu")
+    return types.SimpleNamespace(NeighborList=NeighborList, MultipolarInteraction=MultipolarInteraction, PME=PME,
+                                 Vdw=Vdw, root=root)
+
+
+def water_box_unregistered(name: str, seed: int):
+    """torchff_b200/water.py loaded by path (the box generator only: importing the package
+    would load libtffb200 and register its own torch.ops.torchff schemas)."""
+    import importlib.util
+
+    mod = sys.modules.get("_tff_water")
+    if mod is None:
+        spec = importlib.util.spec_from_file_location(
+            "_tff_water", os.path.join(REPO, "torchff-lib_b200", "torchff_b200", "water.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["_tff_water"] = mod
+        spec.loader.exec_module(mod)
+    return {"water3000": mod.water_box_3000, "water216": mod.water_box_216, "water100k": mod.water_box_100k}[name](seed)
+
+
+def run_reference_cpu(args, ref) -> dict:
+    """The nonbonded part of the reference's TIP3P model (examples/tip3p/model.py:100-133)
+    through the reference's own modules with use_customized_ops=False, FP64, on the host
+    cores: NeighborList._forward_python (torchff/nblist.py:137-140) with the water
+    exclusions, Vdw('LennardJones') with type tables (torchff/vdw.py), rank-0
+    MultipolarInteraction with pairs_excl (torchff/multipoles.py:244-341) and
+    138.935456 x PME(alpha, K, 0) (torchff/pme_ref.py:422-469); energy + backward() for the
+    forces. One step = one full evaluation of the box rank 0 of the other arm evaluates
+    (seed 0). The one-off NeighborList construction (its all-pairs buffer) is timed apart."""
+    import torch
+
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    wb = water_box_unregistered(args.workload, 0)
+    t0 = time.perf_counter()
+    nbl = ref.NeighborList(wb.natoms, exclusions=torch.tensor(wb.nblist_exclusions), use_customized_ops=False)
+    lj = ref.Vdw("LennardJones", cutoff=wb.cutoff, use_customized_ops=False, use_type_pairs=True)
+    coul = ref.MultipolarInteraction(rank=0, cutoff=wb.cutoff, ewald_alpha=wb.alpha, prefactor=138.935456,
+                                     use_customized_ops=False)
+    pme = ref.PME(wb.alpha, wb.grid, 0, use_customized_ops=False)
+    t_init = time.perf_counter() - t0
+    box = torch.tensor(wb.box, dtype=torch.float64)
+    q = torch.tensor(wb.charges, dtype=torch.float64)
+    sig_t = torch.tensor(wb.sigma_table, dtype=torch.float64)
+    eps_t = torch.tensor(wb.epsilon_table, dtype=torch.float64)
+    types_ = torch.tensor(wb.atom_types)
+    excl = torch.tensor(wb.coulomb_exclusions)
+
+    def evaluate():
+        x = torch.tensor(wb.coords, dtype=torch.float64, requires_grad=True)
+        pairs = nbl(x.detach(), box, wb.cutoff)
+        e = (lj(x, pairs, box, sig_t, eps_t, wb.cutoff, atom_types=types_)
+             + coul(x, box, pairs, q, pairs_excl=excl)
+             + pme(x, box, q) * 138.935456)
+        e.backward()
+        return float(e.item()), x.grad
+
+    t0 = time.perf_counter()
+    evaluate()
+    t_first = time.perf_counter() - t0
+    # bounded: the whole arm stays within a few minutes on a host with few cores
+    budget_s = 240.0
+    warm = max(0, min(args.warmup, int(60.0 / max(t_first, 1e-3))) - 1)
+    for _ in range(warm):
+        evaluate()
+    steps = max(1, min(args.steps, int(budget_s / max(t_first, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        energy, _ = evaluate()
+    wall = time.perf_counter() - t0
+    return {"value": steps / wall, "ms_per_step": wall / steps * 1e3, "steps": steps, "warmup": warm + 1,
+            "threads": threads, "init_s": t_init, "energy": energy, "natoms": wb.natoms}
+
+
+def run_reference_gpu(args):
+    """The reference's own compiled CUDA ops (built for sm_100a from its sources into
+    oracle/_ref) on this GPU, FP64 and FP32, CUDA-graph replay of forward + backward as the
+    reference's perf_op does (torchff/test_utils.py:52-146), L2 flushed before each timed
+    step. Runs in a process of its own: the reference's libraries register
+    torch.ops.torchff like libtffb200 does. Rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import glob
+
+    if args.workload not in ("water3000", "water216"):
+        print(json.dumps({"impl": "reference-gpu", "unavailable": f"no reference GPU run for {args.workload}"}))
+        return
+    if not glob.glob(os.path.join(REPO, "oracle", "_ref", "*", "*.so")):
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "the reference's CUDA ops are not built "
+                          "(oracle/_ref is empty; oracle/build_ref.py builds them)"}))
+        return
+    import torch
+
+    from oracle import ref_gpu
+
+    torch.cuda.set_device(0)
+    clocks = ClockSampler(0)
+    clocks.start()
+    clocks.begin()
+    r = ref_gpu.measure(args.workload, max(args.steps, 1), max(args.warmup, 3), check=True)
+    clocks.end()
+    clocks.stop()
+    line = {
+        "impl": "reference-gpu",
+        "metric": METRIC if args.workload == "water3000" else f"{args.workload} PME energy+force evals/s",
+        "value": round(r["fp64_evals_per_s"], 2), "unit": "evals/s", "n_gpus": 1, "steps": max(args.steps, 1),
+        "warmup": max(args.warmup, 3), "ms_per_step": round(r["fp64_ms_per_eval"], 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded TIP3P lattice box, seed 0)",
+        "config": {"workload": f"{args.workload}: {WORKLOAD_TEXT[args.workload]}",
+                   "path": "reference CUDA ops (oracle/_ref): build_neighbor_list_cell_list + "
+                           "compute_lennard_jones_energy (type tables) + compute_multipolar_energy_from_atom_pairs "
+                           "(rank 0, pairs_excl) + 138.935456 x pme_long_range, energy + backward",
+                   "timing": f"{r['fp64_timing_mode']}, {r['l2']}"},
+        "fp64": {"evals_per_s": round(r["fp64_evals_per_s"], 2), "ms_per_eval": round(r["fp64_ms_per_eval"], 5),
+                 "mode": r["fp64_timing_mode"], "energy_rel_err_vs_oracle": r.get("fp64_energy_rel_err_vs_oracle"),
+                 "force_rel_rms_vs_oracle": r.get("fp64_force_rel_rms_vs_oracle")},
+        "fp32": {"evals_per_s": round(r["fp32_evals_per_s"], 2), "ms_per_eval": round(r["fp32_ms_per_eval"], 5),
+                 "mode": r["fp32_timing_mode"], "energy_rel_err_vs_oracle": r.get("fp32_energy_rel_err_vs_oracle"),
+                 "force_rel_rms_vs_oracle": r.get("fp32_force_rel_rms_vs_oracle")},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def reference_gpu_leg(args) -> dict:
+    """Runs the reference-gpu arm in a child process (after our timed regions) and returns
+    its line, or the reason it did not run."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference-gpu", "--workload", args.workload,
+           "--steps", str(min(max(args.steps, 20), 200)), "--warmup", str(max(args.warmup, 3))]
+    env = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        env.pop(k, None)
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "the reference GPU run took longer than 600 s"}
+    for ln in reversed(p.stdout.splitlines()):
+        if ln.startswith("{"):
+            try:
+                return json.loads(ln)
+            except ValueError:
+                break
+    return {"unavailable": f"exit {p.returncode}: {(p.stderr or '').strip().splitlines()[-1:]}"}
+
 
 def _ref_worker_init():
     for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
@@ -687,6 +936,33 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "the reference CPU path keeps an O(N^2) all-pairs "
                           "buffer (~720 GB at 300,000 atoms); not run"}))
         return
+    ref = import_reference_cpu() if args.workload != "serving" else None
+    if ref is not None:
+        r = run_reference_cpu(args, ref)
+        line = {
+            "impl": "reference",
+            "metric": METRIC if args.workload == "water3000" else f"{args.workload} PME energy+force evals/s",
+            "value": round(r["value"], 4), "unit": "evals/s", "n_gpus": args.gpus,
+            "steps": r["steps"], "warmup": r["warmup"], "ms_per_step": round(r["ms_per_step"], 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded TIP3P lattice box, seed 0: the box rank 0 of the other arm evaluates)",
+            "config": {"workload": f"{args.workload}: {WORKLOAD_TEXT[args.workload]}",
+                       "path": "reference torchff (baseline/_ref) pure-torch path: NeighborList + Vdw(LennardJones, "
+                               "type tables) + MultipolarInteraction(rank 0, pairs_excl) + 138.935456 x PME, "
+                               "use_customized_ops=False, FP64, energy + backward()",
+                       "parallelism": f"one process, torch.set_num_threads({r['threads']})",
+                       "one_off_init_s": round(r["init_s"], 3),
+                       "energy_kj_mol": r["energy"]},
+            "cpu_baseline": {"value": round(r["value"], 4), "unit": "evals/s", "cores": r["threads"],
+                             "kind": "reference",
+                             "sample": f"{r['steps']} full evaluations of the {r['natoms']}-atom box (each a step), "
+                                       f"after {r['warmup']} untimed; bounded to ~4 min; NeighborList construction "
+                                       f"({r['init_s']:.1f} s, all-pairs buffer) timed apart"},
+            "e2e": {"value": round(r["value"], 4), "unit": "evals/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
     workers = max(1, min(os.cpu_count() or 1, 16, max(args.steps, 1)))
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers, initializer=_ref_worker_init) as pool:
@@ -708,9 +984,9 @@ def run_reference(args):
         "value": round(value, 4),
         "unit": "systems/s" if serving else "evals/s",
         "n_gpus": args.gpus,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": round(statistics.mean(per) * 1e3, 2),
+        "steps": n_eval,
+        "warmup": len(warm),
+        "ms_per_step": round(wall / n_eval * 1e3, 2),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -730,10 +1006,31 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def free_port() -> int:
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def relaunch_command(argv: list[str], nproc: int, port: int) -> list[str]:
+    """The command that runs this script as `nproc` ranks on this node (one per GPU)."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nproc}",
+            "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + argv
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # started as a plain process: run the N ranks under torch.distributed.run and pass
+        # on their exit status (rank 0 prints the line)
+        cmd = relaunch_command(sys.argv[1:], args.gpus, free_port())
+        raise SystemExit(subprocess.call(cmd))
     if args.impl == "reference":
         run_reference(args)
+    elif args.impl == "reference-gpu":
+        run_reference_gpu(args)
     else:
         run_ours(args)
 

@@ -176,16 +176,18 @@ int tff_nonbonded_atom_pairs(int dtype, int64_t natoms, const void *coords, int6
                              void *workspace, size_t workspace_bytes, tff_stream_t stream);
 
 /* No counterpart in the reference. tff_nonbonded_atom_pairs without a workspace, for
- * callers that cannot allocate device memory: a plugin whose host engine owns every device
- * allocation, work enqueued while a stream capture forbids allocating, or a loop that must
- * not reach an allocator. This entry point calls no cudaMalloc/cudaFree and no allocating
- * library routine; its scratch is a static device array inside libtffb200 (about 3 MiB,
- * held by every GPU that loads the library until exit), so natoms is limited to
- * TFF_NOALLOC_MAX_ATOMS (larger inputs return TFF_ERR_INVALID). The first call on each
- * device looks the array up with cudaGetSymbolAddress: make it before any stream capture.
- * All calls share the array (cleared at the start of each call, it keeps the last call's
- * contents): calls that overlap on the GPU race, so serialise them. Inputs, outputs and
- * results are those of tff_nonbonded_atom_pairs. */
+ * callers that cannot allocate device memory: a force plugin inside a molecular-dynamics
+ * engine that owns every device allocation and gives the plugin only its input and output
+ * buffers, or a time-critical loop that must never reach an allocator (an allocation can
+ * synchronise the device or fail mid-run). This entry point calls no cudaMalloc/cudaFree
+ * and no allocating library routine; its scratch is a static device array inside
+ * libtffb200 (about 3 MiB, held by every GPU that loads the library until exit), so natoms
+ * is limited to TFF_NOALLOC_MAX_ATOMS (larger inputs return TFF_ERR_INVALID). The first
+ * call on each device (and the first after a device reset) looks the array up with
+ * cudaGetSymbolAddress: make it before any stream capture. All calls share the array
+ * (cleared at the start of each call, it keeps the last call's contents): calls that
+ * overlap on the GPU race, so serialise them. Inputs, outputs and results are those of
+ * tff_nonbonded_atom_pairs. */
 #define TFF_NOALLOC_MAX_ATOMS 65536
 int tff_nonbonded_atom_pairs_noalloc(int dtype, int64_t natoms, const void *coords,
                                      int64_t npairs, const int64_t *pairs, const void *box,
@@ -357,7 +359,9 @@ int tff_system_eval(tff_system sys, const void *coords, const void *box, double 
  * synchronises `stream`. coords/box/forces are float64 host arrays whatever the dtype.
  * When coords and forces are page-locked (cudaHostAlloc / cudaHostRegister) the copies and
  * the evaluation are one CUDA-graph launch, kept for the last (coords, forces) pair seen and
- * captured again when either pointer changes. */
+ * captured again when either pointer changes. Returns TFF_ERR_CAPACITY when a cluster's
+ * neighbour list overflowed its capacity (max_cluster_neighbors): the energy and forces it
+ * wrote then miss pairs. */
 int tff_system_eval_host(tff_system sys, const double *coords, const double *box,
                          double *energy, double *forces, tff_stream_t stream);
 /* Device status word of the last evaluation (bit 0: a cluster neighbour list overflowed,

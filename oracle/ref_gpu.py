@@ -102,9 +102,10 @@ def energy(wb, d):
     return e_lj + e_c + e_p
 
 
-def time_graph(wb, d, steps: int, warmup: int = 5) -> tuple[float, str]:
+def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tuple[float, str]:
     """ms per forward + backward: CUDA-graph replay as in torchff/test_utils.py:52-146, or,
-    when the composition cannot be captured, back-to-back eager calls."""
+    when the composition cannot be captured, eager calls. With flush_l2 a 256 MiB device
+    write (larger than the 126 MB L2) runs before every timed replay, outside its events."""
     import torch
 
     x = d["coords"]
@@ -116,8 +117,10 @@ def time_graph(wb, d, steps: int, warmup: int = 5) -> tuple[float, str]:
             energy(wb, d).backward()
     torch.cuda.current_stream().wait_stream(s)
     torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 if flush_l2 else 1, dtype=torch.uint8, device="cuda")
     a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     mode = "cuda_graph"
+    total = 0.0
     try:
         g = torch.cuda.CUDAGraph()
         x.grad = None
@@ -127,58 +130,68 @@ def time_graph(wb, d, steps: int, warmup: int = 5) -> tuple[float, str]:
         for _ in range(warmup):
             g.replay()
         torch.cuda.synchronize()
-        a.record()
-        for _ in range(steps):
-            g.replay()
-        z.record()
+        run = g.replay
     except Exception:  # capture invalidated by a host synchronisation inside an op
         mode = "eager"
         torch.cuda.synchronize()
-        a.record()
-        for _ in range(steps):
+
+        def run():
             x.grad = None
             energy(wb, d).backward()
+    for i in range(steps):
+        flush.fill_(i & 0xff)
+        a.record()
+        run()
         z.record()
-    z.synchronize()
-    return a.elapsed_time(z) / steps, mode
+        z.synchronize()
+        total += a.elapsed_time(z)
+    return total / steps, mode
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="water3000", choices=["water216", "water3000"])
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--check", action="store_true", help="compare the FP64 energy/forces with the oracle")
-    args = ap.parse_args()
+def measure(workload: str = "water3000", steps: int = 200, warmup: int = 5, check: bool = True,
+            flush_l2: bool = True) -> dict:
+    """FP64 and FP32 evaluations of the box (seed 0) through the reference's ops: energy,
+    timing and, with check, the energy and force error against the FP64 oracle."""
     import numpy as np
     import torch
 
     W = water_module()
-    load_reference_ops()
-    wb = {"water216": W.water_box_216, "water3000": W.water_box_3000}[args.workload](0)
-    out = {"workload": args.workload, "natoms": wb.natoms}
+    libs = load_reference_ops()
+    wb = {"water216": W.water_box_216, "water3000": W.water_box_3000}[workload](0)
+    out = {"workload": workload, "natoms": wb.natoms, "libraries": [os.path.relpath(p, REPO) for p in libs],
+           "l2": "flushed before every timed step (256 MiB device write)" if flush_l2 else "not flushed"}
+    forces = {}
     for name, dtype in (("fp64", torch.float64), ("fp32", torch.float32)):
         d = build_inputs(wb, dtype)
         e = energy(wb, d)
         e.backward()
         out[f"{name}_energy"] = float(e.item())
-        out[f"{name}_forces"] = (-d["coords"].grad).double().cpu().numpy()
-        out[f"{name}_ms_per_eval"], out[f"{name}_timing_mode"] = time_graph(wb, d, args.steps)
-        out[f"{name}_evals_per_s"] = 1e3 / out[f"{name}_ms_per_eval"]
-    if args.check:
+        forces[name] = (-d["coords"].grad).double().cpu().numpy()
+        ms, mode = time_graph(wb, d, steps, warmup, flush_l2)
+        out[f"{name}_ms_per_eval"], out[f"{name}_timing_mode"] = ms, mode
+        out[f"{name}_evals_per_s"] = 1e3 / ms
+    if check:
         from oracle import oracle as O
 
         ref = O.fixed_charge_energy(wb.coords, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
                                     wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
                                     138.935456)
         f0 = -ref["grad_coords"]
-        for name in ("fp64", "fp32"):
-            f = out[f"{name}_forces"]
+        for name, f in forces.items():
             out[f"{name}_energy_rel_err_vs_oracle"] = abs(out[f"{name}_energy"] - ref["total"]) / abs(ref["total"])
             out[f"{name}_force_rel_rms_vs_oracle"] = float(np.sqrt(np.mean((f - f0) ** 2)) / np.sqrt(np.mean(f0 ** 2)))
         out["oracle_energy"] = ref["total"]
-    for name in ("fp64", "fp32"):
-        out.pop(f"{name}_forces")
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="water3000", choices=["water216", "water3000"])
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--check", action="store_true", help="compare the energy/forces with the FP64 oracle")
+    ap.add_argument("--no-flush", action="store_true", help="no L2 flush between timed steps")
+    args = ap.parse_args()
+    print(json.dumps(measure(args.workload, args.steps, check=args.check, flush_l2=not args.no_flush)), flush=True)
 
 
 if __name__ == "__main__":

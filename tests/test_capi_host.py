@@ -75,18 +75,23 @@ def test_ctypes_signatures_match_the_header():
         assert [cls(a) for a in argtypes] == args, name
 
 
-def test_integration_ctypes_stub_matches_the_header():
-    """The ctypes stub that the integration guide gives maintainers to paste declares the
-    header's argument types in the header's order."""
-    text = open(os.path.join(REPO, "INTEGRATION.md")).read()
-    stubs = re.findall(r"lib\.(tff_\w+)\.argtypes\s*=\s*\[(.*?)\]", text, flags=re.S)
-    assert stubs
-    kinds = {"c_int": "int", "c_int64": "int64", "c_double": "double", "c_size_t": "size_t", "c_void_p": "ptr",
-             "c_char_p": "ptr"}
+def test_example_ctypes_stub_matches_the_header():
+    """The ctypes stub a maintainer adds (torchff_b200/capi_example.py) declares the header's
+    return and argument types in the header's order, on the built library."""
+    import ctypes as C
+
+    from torchff_b200 import capi_example
+
+    kinds = {C.c_int: "int", C.c_int64: "int64", C.c_double: "double", C.c_size_t: "size_t", C.c_void_p: "ptr",
+             C.c_char_p: "ptr"}
     protos = _header_prototypes()
-    for name, body in stubs:
-        args = [kinds[a.strip().split(".")[-1]] for a in body.split(",") if a.strip()]
-        assert args == protos[name][1], name
+    lib = capi_example.load()
+    declared = ["tff_pairs_workspace_bytes", "tff_last_error", "tff_nonbonded_atom_pairs"]
+    for name in declared:
+        fn = getattr(lib, name)
+        ret, args = protos[name]
+        assert kinds[fn.restype] == ret, name
+        assert [kinds[a] for a in fn.argtypes] == args, name
 
 
 def test_bench_throughput_fields():

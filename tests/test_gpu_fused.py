@@ -194,6 +194,34 @@ def test_empty_system():
         assert sysm.status() == 0
 
 
+def test_cluster_list_overflow_is_reported(ref216):
+    """A neighbour-cluster capacity far below what the box needs (4 clusters, where the
+    216-water box's clusters see ~20) drops pairs: the host entry point returns
+    TFF_ERR_CAPACITY (RuntimeError), evaluate() raises when check_status is on, and the status
+    word says so; the same system with the default capacity evaluates without an error."""
+    import torchff_b200._lib as L
+    from torchff_b200.system import FixedChargeSystem
+
+    wb, _ = ref216
+    for pinned in (False, True):
+        small = FixedChargeSystem.from_water_box(wb, dtype=torch.float32, max_cluster_neighbors=4, check_status=True)
+        x = torch.tensor(wb.coords, dtype=torch.float64)
+        b = torch.tensor(wb.box, dtype=torch.float64)
+        f = torch.zeros_like(x)
+        if pinned:
+            x, b, f = x.pin_memory(), b.pin_memory(), f.pin_memory()
+        with pytest.raises(RuntimeError, match="overflow"):
+            small.evaluate_host(x, b, f)
+        assert L.TFF_ERR_CAPACITY == 5 and small.status() & 1
+    with pytest.raises(RuntimeError, match="overflow"):
+        small.evaluate(t(wb.coords, torch.float32), t(wb.box, torch.float32))
+    ok = FixedChargeSystem.from_water_box(wb, dtype=torch.float32, check_status=True)
+    f = np.zeros_like(wb.coords)
+    ok.evaluate_host(np.ascontiguousarray(wb.coords), np.ascontiguousarray(wb.box), f)
+    ok.evaluate(t(wb.coords, torch.float32), t(wb.box, torch.float32))
+    assert ok.status() == 0
+
+
 def test_host_entry_point_matches_device(ref216):
     from torchff_b200.system import FixedChargeSystem
 

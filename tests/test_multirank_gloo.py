@@ -84,3 +84,33 @@ def test_frame_sharded_gradient_allreduce_matches_single_process(tmp_path):
     ref = _frame_grads(range(NFRAMES))
     for a, b in zip(res["grads"], ref):
         assert torch.allclose(a, b, rtol=1e-12, atol=1e-12 * float(b.abs().max()))
+
+
+def test_bench_starts_its_own_ranks(tmp_path):
+    """`python bench.py --gpus 2` started as a plain process re-runs itself as 2 ranks under
+    torch.distributed.run (127.0.0.1); rank 0 prints the one JSON line and the other rank
+    exits 0. Driven through the reference arm's quick path (the 300,000-atom workload it does
+    not run), which needs no GPU."""
+    import json
+    import subprocess
+    import sys
+
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    p = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--gpus", "2", "--impl", "reference",
+                        "--workload", "water100k", "--steps", "1", "--warmup", "1"],
+                       capture_output=True, text=True, timeout=300, env=env, cwd=str(tmp_path))
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [json.loads(ln) for ln in p.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1 and lines[0]["impl"] == "reference" and "unavailable" in lines[0]
+
+
+def test_bench_relaunch_command():
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(REPO, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    cmd = bench.relaunch_command(["--gpus", "4", "--steps", "3"], 4, 29501)
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in cmd and cmd[cmd.index("--master-addr") + 1] == "127.0.0.1"
+    assert cmd[-3:] == ["--gpus", "4", "--steps", "3"][-3:] and cmd[cmd.index("--master-port") + 1] == "29501"

@@ -1,13 +1,16 @@
-"""tff_nonbonded_atom_pairs_noalloc against tff_nonbonded_atom_pairs, both through the C ABI.
+"""tff_nonbonded_atom_pairs_noalloc against tff_nonbonded_atom_pairs, both through the C ABI,
+and against the reference's own values for the same inputs (golden pairs_random.npz).
 
-The no-alloc entry point serves callers that may not allocate device memory (a plugin
-whose host engine owns all allocations, or code enqueuing work during a stream capture):
-it keeps its scratch in a static device array of libtffb200 instead of a caller
-workspace. This file is collected last so a run that stops at the first failure has run
-every other test; it also passes alone in a fresh process.
+The no-alloc entry point serves callers that may not allocate device memory (a force
+plugin whose host MD engine owns all allocations, or a time-critical loop that must never
+reach an allocator): it keeps its scratch in a static device array of libtffb200 instead
+of a caller workspace. This file is collected last so a run that stops at the first
+failure has run every other test; it also passes alone in a fresh process.
 
-Tolerances are those of the pair-term tests: FP64 energies 1e-11 relative, gradients
-1e-9 of their max magnitude; mixed precision 2e-6 and 1e-5.
+Tolerances are those of the pair-term tests: against the workspace entry point FP64
+energies 1e-11 relative, gradients 1e-9 of their max magnitude, mixed precision 2e-6 and
+1e-5; against the golden values FP64 1e-11 / 1e-9 and mixed 1e-5 / 1e-5 (rounding the FP64
+inputs to FP32 bounds the mixed energies).
 """
 import ctypes
 import os
@@ -21,6 +24,7 @@ from conftest import GOLDEN
 pytestmark = pytest.mark.gpu
 
 TOL = {torch.float64: (1e-11, 1e-9), torch.float32: (2e-6, 1e-5)}
+GOLDEN_TOL = {torch.float64: (1e-11, 1e-9), torch.float32: (1e-5, 1e-5)}
 
 
 def _rel_max(a, b):
@@ -63,11 +67,16 @@ def test_noalloc_matches_workspace_entry_point_twice(dtype):
     lib = L.lib
     ref = _call(lib, lib.tff_nonbonded_atom_pairs, g, dtype, with_workspace=True)
     etol, gtol = TOL[dtype]
+    getol, ggtol = GOLDEN_TOL[dtype]
     for _ in range(2):  # the shared static scratch must be cleared between calls
         got = _call(lib, lib.tff_nonbonded_atom_pairs_noalloc, g, dtype, with_workspace=False)
         assert abs(got["energy"].item() - ref["energy"].item()) <= etol * abs(ref["energy"].item())
         for k in ("gx", "gs", "ge", "gq"):
             assert _rel_max(got[k], ref[k]) < gtol, k
+        # the reference's own result (shifted Coulomb + LJ with Lorentz-Berthelot combining)
+        assert abs(got["energy"].item() - g["shift_energy"]) <= getol * abs(g["shift_energy"])
+        for k in ("gx", "gs", "ge", "gq"):
+            assert _rel_max(got[k], torch.tensor(g[f"shift_{k}"])) < ggtol, k
 
 
 def test_noalloc_rejects_sizes_beyond_the_static_limit():

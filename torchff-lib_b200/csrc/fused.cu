@@ -94,7 +94,7 @@ int launch_bonded(tff_system sys, const T *x, cudaStream_t s) {
 
 template <class T>
 int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T *forces, double *forces64, T *grad_q,
-                     double *terms, cudaStream_t s, cudaEvent_t *ev = nullptr) {
+                     double *terms, cudaStream_t s, cudaEvent_t *ev = nullptr, unsigned *status_out = nullptr) {
   using S = typename Acc<T>::S;
   const int64_t n = sys->desc.natoms;
   auto mark = [&](int k, cudaStream_t st) { return ev ? record_event(ev[k], st) : TFF_OK; };
@@ -184,7 +184,8 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
                 use_pme ? static_cast<const T *>(sys->pme_grad) : static_cast<const T *>(nullptr),
                 use_pme ? static_cast<const T *>(sys->pme_phi) : static_cast<const T *>(nullptr), forces, forces64,
                 grad_q, static_cast<const S *>(energies), e_pme, sys->desc.coul_constant, energy, terms, 1,
-                sys->has_bonded() && n > 0 ? static_cast<const S *>(sys->bacc) : static_cast<const S *>(nullptr));
+                sys->has_bonded() && n > 0 ? static_cast<const S *>(sys->bacc) : static_cast<const S *>(nullptr),
+                status_out);
   if (st != TFF_OK) return st;
   return mark(5, s);
 }
@@ -586,9 +587,11 @@ int capture_host_graph(tff_system sys, const double *coords, double *forces, con
   const double *x_in = stage, *box_in = stage + 3 * n;
   double *e_out = sys->dev_e, *f_out = sys->dev_f;
   const bool zero_copy = coords && 3 * n * (int64_t)sizeof(double) <= kZeroCopyMaxBytes;
+  double *io = nullptr;
+  TFF_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&io), sys->pinned_io, 0));
+  // the finalize kernel writes the build's overflow word next to the energy slot
+  unsigned *status_out = reinterpret_cast<unsigned *>(io + 10);
   if (zero_copy) {
-    double *io = nullptr;
-    TFF_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&io), sys->pinned_io, 0));
     x_in = dcoords;
     box_in = io;
     e_out = io + 9;
@@ -610,11 +613,13 @@ int capture_host_graph(tff_system sys, const double *coords, double *forces, con
     if (sys->desc.dtype == TFF_F32) {
       float *x = static_cast<float *>(sys->dev_x);
       cast_inputs_kernel<float><<<nb, 256, 0, cs>>>(x_in, box_in, x, x + 3 * n, 3 * n);
-      st = system_eval_impl<float>(sys, x, x + 3 * n, e_out, nullptr, f_out, nullptr, nullptr, cs);
+      st = system_eval_impl<float>(sys, x, x + 3 * n, e_out, nullptr, f_out, nullptr, nullptr, cs, nullptr,
+                                    status_out);
     } else {
       double *x = static_cast<double *>(sys->dev_x);
       cast_inputs_kernel<double><<<nb, 256, 0, cs>>>(x_in, box_in, x, x + 3 * n, 3 * n);
-      st = system_eval_impl<double>(sys, x, x + 3 * n, e_out, nullptr, f_out, nullptr, nullptr, cs);
+      st = system_eval_impl<double>(sys, x, x + 3 * n, e_out, nullptr, f_out, nullptr, nullptr, cs, nullptr,
+                                     status_out);
     }
   }
   if (coords && !zero_copy && st == TFF_OK && ce == cudaSuccess) {
@@ -634,6 +639,18 @@ int capture_host_graph(tff_system sys, const double *coords, double *forces, con
   if (ie != cudaSuccess) {
     *out = nullptr;
     return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+  }
+  return TFF_OK;
+}
+
+// Status of the evaluation tff_system_eval_host just waited for: the build's overflow word
+// that its finalize kernel copied into the page-locked slot.
+int host_status(tff_system sys) {
+  unsigned w = 0;
+  std::memcpy(&w, sys->pinned_io + 10, sizeof(w));
+  if (w & 1u) {
+    set_error("a cluster's neighbour list overflowed its capacity (max_cluster_neighbors): pairs were dropped");
+    return TFF_ERR_CAPACITY;
   }
   return TFF_OK;
 }
@@ -667,8 +684,8 @@ int tff_system_eval_host(tff_system sys, const double *coords, const double *box
   const void *dcoords = n > 0 ? mapped_address(coords) : nullptr;
   void *dforces = dcoords ? mapped_address(forces) : nullptr;
   const bool pinned = dcoords != nullptr && dforces != nullptr;
+  if (sys->pinned_io == nullptr) TFF_CUDA(cudaHostAlloc(&sys->pinned_io, 16 * sizeof(double), cudaHostAllocMapped));
   if (pinned && (sys->pinned_graph == nullptr || sys->pinned_ptrs[0] != coords || sys->pinned_ptrs[1] != forces)) {
-    if (sys->pinned_io == nullptr) TFF_CUDA(cudaHostAlloc(&sys->pinned_io, 16 * sizeof(double), cudaHostAllocMapped));
     if (sys->pinned_graph) {
       cudaGraphExecDestroy(sys->pinned_graph);
       sys->pinned_graph = nullptr;
@@ -684,7 +701,7 @@ int tff_system_eval_host(tff_system sys, const double *coords, const double *box
     TFF_CUDA(cudaGraphLaunch(sys->pinned_graph, s));
     TFF_CUDA(cudaStreamSynchronize(s));
     *energy = sys->pinned_io[9];
-    return TFF_OK;
+    return host_status(sys);
   }
   // Other buffers: the device part is captured once (it touches only the system's own
   // buffers) and the copies are issued around it.
@@ -698,7 +715,7 @@ int tff_system_eval_host(tff_system sys, const double *coords, const double *box
   if (n > 0) TFF_CUDA(cudaMemcpyAsync(forces, sys->dev_f, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   TFF_CUDA(cudaMemcpyAsync(energy, sys->dev_e, sizeof(double), cudaMemcpyDeviceToHost, s));
   TFF_CUDA(cudaStreamSynchronize(s));
-  return TFF_OK;
+  return host_status(sys);
 }
 
 int tff_timer_create(tff_timer *timer) {

@@ -12,6 +12,8 @@
 
 #include <mutex>
 
+#include <cuda.h>   // driver types only: cuCtxGetCurrent / cuCtxGetId are reached via the runtime
+
 #include "tff_common.cuh"
 
 namespace tff {
@@ -355,20 +357,55 @@ constexpr int64_t kNoAllocMaxAtoms = TFF_NOALLOC_MAX_ATOMS;
 constexpr size_t kNoAllocScratchBytes = (size_t)kNoAllocMaxAtoms * 6 * 8 + 8192 * 8 + 512;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of g_noalloc_scratch on the current device. In host code the symbol is
-// only a host-side stand-in, so the address is looked up once per device with
-// cudaGetSymbolAddress (with that device current) and cached.
+// Id of the context current on this thread (0 while none is), through the driver's
+// cuCtxGetCurrent / cuCtxGetId reached via the runtime (the library does not link the driver
+// library). Context ids are unique for the life of the process, so the context the runtime
+// creates after a cudaDeviceReset never carries the id of the one it replaced.
+int current_context_id(unsigned long long *id) {
+  using GetCurrent = CUresult (*)(CUcontext *);
+  using GetId = CUresult (*)(CUcontext, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  if (get_current == nullptr || get_id == nullptr) {
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult r1 = cudaDriverEntryPointSymbolNotFound, r2 = r1;
+    TFF_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &r1));
+    TFF_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &r2));
+    TFF_ARG(r1 == cudaDriverEntryPointSuccess && r2 == cudaDriverEntryPointSuccess && f1 && f2,
+            "the driver offers no cuCtxGetCurrent/cuCtxGetId");
+    get_current = reinterpret_cast<GetCurrent>(f1);
+    get_id = reinterpret_cast<GetId>(f2);
+  }
+  CUcontext ctx = nullptr;
+  TFF_ARG(get_current(&ctx) == CUDA_SUCCESS, "cuCtxGetCurrent failed");
+  *id = 0;
+  if (ctx != nullptr) TFF_ARG(get_id(ctx, id) == CUDA_SUCCESS, "cuCtxGetId failed");
+  return TFF_OK;
+}
+
+// Device address of g_noalloc_scratch in the current device's context. In host code the
+// symbol is only a host-side stand-in, so the address is looked up with
+// cudaGetSymbolAddress (with that device current) at the first call on each device, and
+// again whenever the device's context has changed since (after a cudaDeviceReset, the
+// old address belongs to a destroyed context).
 int noalloc_scratch(void **out) {
   static std::mutex mu;
   static void *addr[64] = {nullptr};
+  static unsigned long long ctx_of[64] = {0};
   int dev = 0;
   TFF_CUDA(cudaGetDevice(&dev));
   TFF_ARG(dev >= 0 && dev < 64, "device index %d out of range", dev);
   std::lock_guard<std::mutex> lock(mu);
-  if (addr[dev] == nullptr) {
+  unsigned long long ctx = 0;
+  int st = current_context_id(&ctx);
+  if (st != TFF_OK) return st;
+  if (addr[dev] == nullptr || ctx == 0 || ctx != ctx_of[dev]) {
     void *p = nullptr;
-    TFF_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    TFF_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));   // makes the context current if none was
+    st = current_context_id(&ctx);
+    if (st != TFF_OK) return st;
     addr[dev] = p;
+    ctx_of[dev] = ctx;
   }
   *out = addr[dev];
   return TFF_OK;
@@ -382,15 +419,17 @@ using namespace tff;
 extern "C" {
 
 // Same computation as tff_nonbonded_atom_pairs, for callers that cannot allocate device
-// memory: a plugin running inside a host engine that owns every device allocation, code
-// that enqueues work while a CUDA stream capture forbids allocation, or a loop that must
-// never reach an allocator. Scratch is the library's static device array instead of a
-// caller workspace; the caller still passes inputs and outputs. Limits and sharing:
+// memory: a force plugin inside a molecular-dynamics engine that owns every device
+// allocation and hands the plugin only its input and output buffers, or a time-critical
+// loop that must never reach an allocator (an allocation can synchronise the device or
+// fail mid-run). Scratch is the library's static device array instead of a caller
+// workspace; the caller still passes inputs and outputs. Limits and sharing:
 // natoms <= TFF_NOALLOC_MAX_ATOMS (larger sizes return TFF_ERR_INVALID); the first call on
-// each device looks the array up with cudaGetSymbolAddress, so make that first call before
-// any stream capture; all calls share the one array (its accumulators are cleared at the
-// start of every call and it keeps the last call's contents), so calls that overlap on the
-// GPU, e.g. on two streams at once, race and must be serialised by the caller.
+// each device (and the first after a device reset) looks the array up with
+// cudaGetSymbolAddress, so make that first call before any stream capture; all calls share
+// the one array (its accumulators are cleared at the start of every call and it keeps the
+// last call's contents), so calls that overlap on the GPU, e.g. on two streams at once,
+// race and must be serialised by the caller.
 int tff_nonbonded_atom_pairs_noalloc(int dtype, int64_t natoms, const void *coords, int64_t npairs,
                                      const int64_t *pairs, const void *box, const void *sigma,
                                      const void *epsilon, const void *charges, double coul_constant,

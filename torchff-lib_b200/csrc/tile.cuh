@@ -600,8 +600,11 @@ __global__ void finalize_kernel(ClusterData<T> cl, const typename Acc<T>::S *gx,
                                 const T *pme_grad, const T *pme_phi, T *forces, double *forces64, T *grad_q,
                                 const typename Acc<T>::S *e_tile_acc, const double *e_pme, double kc,
                                 double *energy, double *terms, int nsys,
-                                const typename Acc<T>::S *bonded = nullptr) {
+                                const typename Acc<T>::S *bonded = nullptr, unsigned *status_out = nullptr) {
   pdl_enter();
+  // the build's overflow word (bit 0: a cluster's neighbour list was cut at its capacity),
+  // copied out for a host caller that reads it together with the energy
+  if (status_out && blockIdx.x == 0 && threadIdx.x == 0) *status_out = cl.status[0];
   for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < cl.natoms;
        a += (int64_t)gridDim.x * blockDim.x) {
     const int64_t s = cl.inv[a];

@@ -29,7 +29,12 @@ COULOMB_PREFACTOR = 138.935456
 class FixedChargeSystem:
     def __init__(self, charges, sigma, epsilon, exclusions, cutoff: float, ewald_alpha: float, pme_grid: int,
                  coul_constant: float = COULOMB_PREFACTOR, dtype: torch.dtype = torch.float32,
-                 device: torch.device | str = "cuda", max_cluster_neighbors: int = 0):
+                 device: torch.device | str = "cuda", max_cluster_neighbors: int = 0, check_status: bool = False):
+        """check_status: after every evaluate() / evaluate_grads() (and so every module
+        forward), wait for the device and raise if a cluster's neighbour list overflowed its
+        capacity (pairs dropped). Off by default: the check synchronises. evaluate_host
+        always checks (it synchronises anyway); evaluate_into never does (graph capture)."""
+        self.check_status = bool(check_status)
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("FixedChargeSystem needs a CUDA device")
@@ -135,6 +140,7 @@ class FixedChargeSystem:
         et = torch.empty(6 if getattr(self, "nbonded_terms", 0) else 4, dtype=torch.float64,
                          device=self.device) if terms else None
         self.evaluate_into(x, b, energy, forces, gq, et)
+        self._check_overflow()
         out = {"energy": energy[0], "forces": forces}
         if gq is not None:
             out["grad_charges"] = gq
@@ -166,8 +172,14 @@ class FixedChargeSystem:
         L.check(L.lib.tff_system_eval_grads(self._h, L.ptr(x), L.ptr(b), L.ptr(out["energy"]), L.ptr(out["forces"]),
                                             L.ptr(out["grad_charges"]), L.ptr(out["grad_sigma"]),
                                             L.ptr(out["grad_epsilon"]), self._stream()), "tff_system_eval_grads")
+        self._check_overflow()
         out["energy"] = out["energy"][0]
         return out
+
+    def _check_overflow(self) -> None:
+        if self.check_status and self.status() & 1:
+            raise RuntimeError("FixedChargeSystem: a cluster's neighbour list overflowed its capacity "
+                               "(max_cluster_neighbors); pairs were dropped")
 
     def hvp(self, coords: torch.Tensor, box: torch.Tensor, direction: torch.Tensor) -> dict:
         """Derivatives of s = sum_i u_i . dE/dx_i (u = `direction`, (N,3)) with respect to the
