@@ -502,3 +502,160 @@ def fixed_charge_energy(coords, box, charges, sigma_table, epsilon_table, atom_t
         "grad_charges": gq_c + prefactor * pot,
         "pairs": pairs,
     }
+
+
+# ---------------------------------------------------------------------------
+# large orthorhombic boxes: the same energy and forces without an O(N^2) pair list
+# ---------------------------------------------------------------------------
+
+
+def _real_pair_terms(r, qq, sig, eps, alpha, prefactor):
+    """Per pair: LJ 12-6 (torchff/vdw.py:86-111) + prefactor q_i q_j erfc(a r)/r
+    (torchff/multipoles.py:244-341, rank 0) and dE/dr."""
+    e_lj, de_lj, _, _ = _lj_terms(r, np.where(sig > 0, sig, 1.0), eps)
+    u = alpha * r
+    ec = _erfc(u)
+    e_c = prefactor * qq * ec / r
+    de_c = prefactor * qq * (-ec / r**2 - (2.0 * alpha / math.sqrt(math.pi)) * np.exp(-u * u) / r)
+    return e_lj + e_c, de_lj + de_c
+
+
+def real_space_cells(coords, box, q, atom_types, sigma_table, epsilon_table, coulomb_excl, cutoff, alpha,
+                     prefactor):
+    """Total real-space energy (LJ with type tables + Ewald real space with the erfc-1
+    exclusion correction) of an orthorhombic box with at least 3 cells of edge >= cutoff per
+    axis, by cell binning: every pair within the cutoff is visited once through the cell
+    and its 13 forward neighbour cells. Same sums as ``lennard_jones`` + ``ewald_real`` over
+    the half neighbour list (``torchff/nblist.py:137-140``, exclusions removed), with the
+    excluded pairs' correction of ``torchff/multipoles.py:312-341``."""
+    coords = np.asarray(coords, np.float64)
+    L = np.diag(np.asarray(box, np.float64))
+    nc = np.floor(L / cutoff).astype(np.int64)
+    assert np.all(nc >= 3) and np.allclose(box, np.diag(L)), "orthorhombic box, >= 3 cells per axis"
+    frac = coords / L
+    frac -= np.floor(frac)
+    cidx = np.minimum((frac * nc).astype(np.int64), nc - 1)
+    flat = (cidx[:, 0] * nc[1] + cidx[:, 1]) * nc[2] + cidx[:, 2]
+    order = np.argsort(flat, kind="stable")
+    start = np.searchsorted(flat[order], np.arange(nc.prod() + 1))
+    x = coords[order]
+    qs = np.asarray(q, np.float64)[order]
+    ts = np.asarray(atom_types)[order]
+    offs = [(a, b, c) for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1) if (a, b, c) > (0, 0, 0)]
+    rc2 = cutoff * cutoff
+    energy = 0.0
+    for cx in range(nc[0]):
+        for cy in range(nc[1]):
+            for cz in range(nc[2]):
+                c0 = (cx * nc[1] + cy) * nc[2] + cz
+                a = np.arange(start[c0], start[c0 + 1])
+                for off in [(0, 0, 0)] + offs:
+                    c1 = (((cx + off[0]) % nc[0]) * nc[1] + (cy + off[1]) % nc[1]) * nc[2] + (cz + off[2]) % nc[2]
+                    b = np.arange(start[c1], start[c1 + 1])
+                    d = x[a][:, None, :] - x[b][None, :, :]
+                    d -= L * np.floor(d / L + 0.5)
+                    r2 = np.einsum("abk,abk->ab", d, d)
+                    m = r2 <= rc2
+                    if off == (0, 0, 0):
+                        m &= a[:, None] < b[None, :]
+                    ia, ib = np.nonzero(m)
+                    if ia.size == 0:
+                        continue
+                    i, j = a[ia], b[ib]
+                    r = np.sqrt(r2[ia, ib])
+                    e, _ = _real_pair_terms(r, qs[i] * qs[j], sigma_table[ts[i], ts[j]], epsilon_table[ts[i], ts[j]],
+                                            alpha, prefactor)
+                    energy += float(np.sum(e))
+    # excluded pairs: take out the pair terms counted above, add the correction
+    ex = np.asarray(coulomb_excl, np.int64)
+    qv = np.asarray(q, np.float64)
+    tv = np.asarray(atom_types)
+    d = min_image(coords[ex[:, 0]] - coords[ex[:, 1]], box)
+    r = np.sqrt(np.einsum("ab,ab->a", d, d))
+    m = r <= cutoff
+    i, j, r = ex[m, 0], ex[m, 1], r[m]
+    e_in, _ = _real_pair_terms(r, qv[i] * qv[j], sigma_table[tv[i], tv[j]], epsilon_table[tv[i], tv[j]], alpha,
+                               prefactor)
+    corr = prefactor * qv[i] * qv[j] * (_erfc(alpha * r) - 1.0) / r
+    return energy - float(np.sum(e_in)) + float(np.sum(corr))
+
+
+def real_space_grad_subset(coords, box, q, atom_types, sigma_table, epsilon_table, coulomb_excl, cutoff, alpha,
+                           prefactor, subset, chunk: int = 16):
+    """dE/dx of the real-space energy of ``real_space_cells`` for the atoms ``subset``, from
+    their distances to every atom (minimum image of an orthorhombic box)."""
+    coords = np.asarray(coords, np.float64)
+    qv = np.asarray(q, np.float64)
+    tv = np.asarray(atom_types)
+    L = np.diag(np.asarray(box, np.float64))
+    ex = np.asarray(coulomb_excl, np.int64)
+    subset = np.asarray(subset, np.int64)
+    out = np.zeros((subset.size, 3))
+    for c0 in range(0, subset.size, chunk):
+        s = subset[c0:c0 + chunk]
+        d = coords[s][:, None, :] - coords[None, :, :]
+        d -= L * np.floor(d / L + 0.5)
+        r2 = np.einsum("abk,abk->ab", d, d)
+        m = (r2 <= cutoff * cutoff) & (np.arange(coords.shape[0])[None, :] != s[:, None])
+        for k_, a in enumerate(s):
+            partners = np.concatenate([ex[ex[:, 0] == a, 1], ex[ex[:, 1] == a, 0]])
+            m[k_, partners] = False
+        ia, jb = np.nonzero(m)
+        r = np.sqrt(r2[ia, jb])
+        i = s[ia]
+        _, dedr = _real_pair_terms(r, qv[i] * qv[jb], sigma_table[tv[i], tv[jb]], epsilon_table[tv[i], tv[jb]],
+                                   alpha, prefactor)
+        g = (dedr / r)[:, None] * d[ia, jb]
+        np.add.at(out, c0 + ia, g)
+        for k_, a in enumerate(s):   # excluded partners: the erfc-1 correction only
+            partners = np.concatenate([ex[ex[:, 0] == a, 1], ex[ex[:, 1] == a, 0]])
+            dd = min_image(coords[a] - coords[partners], box)
+            rr = np.sqrt(np.einsum("ab,ab->a", dd, dd))
+            keep = rr <= cutoff
+            dd, rr, p = dd[keep], rr[keep], partners[keep]
+            u = alpha * rr
+            damp = _erfc(u) - 1.0
+            dfdr = -damp / rr**2 - (2.0 * alpha / math.sqrt(math.pi)) * np.exp(-u * u) / rr
+            out[c0 + k_] += np.sum((prefactor * qv[a] * qv[p] * dfdr / rr)[:, None] * dd, axis=0)
+    return out
+
+
+def pme_subset(coords, box, q, alpha, K, subset):
+    """``pme`` (energy incl. self term) with dE/dx gathered for the atoms ``subset`` only;
+    the charge grid is spread from every atom with a weighted bincount (large N)."""
+    coords = np.asarray(coords, np.float64)
+    q = np.asarray(q, np.float64)
+    n = coords.shape[0]
+    grid = np.zeros(K * K * K)
+    for c0 in range(0, n, 65536):
+        sl = slice(c0, min(n, c0 + 65536))
+        _, m0, val, _, shifts = _pme_stencil(coords[sl], box, K)
+        idx = (m0[:, :, None] + shifts[None, None, :]) % K
+        w3 = val[:, 0, :, None, None] * val[:, 1, None, :, None] * val[:, 2, None, None, :]
+        flat = idx[:, 0, :, None, None] * K * K + idx[:, 1, None, :, None] * K + idx[:, 2, None, None, :]
+        grid += np.bincount(flat.reshape(-1), weights=(q[sl, None, None, None] * w3).reshape(-1), minlength=K ** 3)
+    grid = grid.reshape(K, K, K)
+    S = np.fft.fftn(grid)
+    f = signed_frequency(K).astype(np.float64)
+    mx, my, mz = np.meshgrid(f, f, f, indexing="ij")
+    kvec = 2.0 * np.pi * (np.stack([mx, my, mz], -1) @ np.linalg.inv(box).T)
+    ksq = np.sum(kvec * kvec, -1)
+    vol = abs(np.linalg.det(box))
+    th = bspline_moduli(K)
+    theta = th[:, None, None] * th[None, :, None] * th[None, None, :]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        C = 4.0 * np.pi / vol / ksq * np.exp(-ksq / (4.0 * alpha * alpha))
+    C[0, 0, 0] = 0.0
+    Phi = np.real(np.fft.ifftn(C * S / (theta * theta), norm="forward"))
+    energy = 0.5 * float(np.sum(grid * Phi)) - alpha / math.sqrt(math.pi) * float(np.sum(q * q))
+    subset = np.asarray(subset, np.int64)
+    recip, m0, val, der, shifts = _pme_stencil(coords[subset], box, K)
+    idx = (m0[:, :, None] + shifts[None, None, :]) % K
+    flat = idx[:, 0, :, None, None] * K * K + idx[:, 1, None, :, None] * K + idx[:, 2, None, None, :]
+    loc = Phi.reshape(-1)[flat]
+    gu = np.stack([
+        np.sum(loc * der[:, 0, :, None, None] * val[:, 1, None, :, None] * val[:, 2, None, None, :], (1, 2, 3)),
+        np.sum(loc * val[:, 0, :, None, None] * der[:, 1, None, :, None] * val[:, 2, None, None, :], (1, 2, 3)),
+        np.sum(loc * val[:, 0, :, None, None] * val[:, 1, None, :, None] * der[:, 2, None, None, :], (1, 2, 3)),
+    ], 1)
+    return energy, q[subset, None] * (-(gu @ recip))

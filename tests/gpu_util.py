@@ -34,3 +34,25 @@ def canon(pairs: torch.Tensor, npairs: torch.Tensor | None = None) -> np.ndarray
     if npairs is not None:
         p = p[: int(npairs.item())]
     return O.canonical_pairs(p)
+
+
+def oracle_water(wb, coords=None, flexible: bool = False) -> dict:
+    """The FP64 oracle of a water box's nonbonded model (LJ type tables + real-space Ewald with
+    exclusion correction + 138.935456 x PME), plus the harmonic O-H bonds and H-O-H angles
+    when ``flexible``: total energy, dE/dx, and the summed magnitudes of the terms (the scale
+    of the mixed-precision energy tolerance)."""
+    from oracle import oracle as O
+    from torchff_b200.water import water_bonded_terms
+
+    x = wb.coords if coords is None else coords
+    ref = O.fixed_charge_energy(x, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
+                                wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
+                                138.935456)
+    e, g = ref["total"], ref["grad_coords"].copy()
+    scale = abs(ref["lj"]) + abs(ref["coul_real"]) + abs(138.935456 * ref["pme_raw"])
+    if flexible:
+        bt = water_bonded_terms(wb.n_waters)
+        eb, gb = O.harmonic_bond(x, bt.bonds, bt.b0, bt.kb)[:2]
+        ea, ga = O.harmonic_angle(x, bt.angles, bt.th0, bt.kth)[:2]
+        e, g, scale = e + eb + ea, g + gb + ga, scale + abs(eb) + abs(ea)
+    return {"energy": e, "grad": g, "scale": scale}

@@ -5,7 +5,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, REPO
 from oracle import oracle as O
 
 
@@ -104,3 +104,28 @@ def test_bonded_water():
     assert abs(e - float(g["angle_energy"])) <= 1e-13 * abs(float(g["angle_energy"]))
     assert _rel(gx, g["angle_gx"]) < 1e-12 and _rel(gt, g["angle_gth0"]) < 1e-12 and _rel(gk, g["angle_gk"]) < 1e-12
     assert np.max(np.abs(O.angles(g["coords"], g["angles"]) - g["theta"])) < 1e-14
+
+
+def test_large_box_oracle_matches_pair_list_oracle():
+    """The cell-binned real-space energy, the sampled-atom real-space gradients and the
+    sampled PME of the oracle (used for the 300,000-atom box) equal the pair-list oracle on
+    the 3000-water box."""
+    import sys
+
+    sys.path.insert(0, os.path.join(REPO, "torchff-lib_b200"))
+    from torchff_b200.water import water_box_3000
+
+    wb = water_box_3000(0)
+    ref = O.fixed_charge_energy(wb.coords, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
+                                wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid, 138.935456)
+    e_real = O.real_space_cells(wb.coords, wb.box, wb.charges, wb.atom_types, wb.sigma_table, wb.epsilon_table,
+                                wb.coulomb_exclusions, wb.cutoff, wb.alpha, 138.935456)
+    assert abs(e_real - (ref["lj"] + ref["coul_real"])) < 1e-11 * (abs(ref["lj"]) + abs(ref["coul_real"]))
+    subset = np.random.default_rng(5).choice(wb.natoms, 40, replace=False)
+    e_pme, g_pme = O.pme_subset(wb.coords, wb.box, wb.charges, wb.alpha, wb.grid, subset)
+    assert abs(e_pme - ref["pme_raw"]) < 1e-11 * abs(ref["pme_raw"])
+    g_real = O.real_space_grad_subset(wb.coords, wb.box, wb.charges, wb.atom_types, wb.sigma_table,
+                                      wb.epsilon_table, wb.coulomb_exclusions, wb.cutoff, wb.alpha, 138.935456, subset)
+    g = g_real + 138.935456 * g_pme
+    gref = ref["grad_coords"][subset]
+    assert np.max(np.abs(g - gref)) < 1e-10 * np.max(np.abs(gref))

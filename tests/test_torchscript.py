@@ -11,6 +11,7 @@ import pytest
 import torch
 
 from conftest import REPO
+from gpu_util import oracle_water, rel_rms
 
 
 def test_class_registers_and_pickles_without_gpu(tmp_path):
@@ -45,6 +46,11 @@ def test_scripted_model_matches_python_path(tmp_path, flexible):
     # same library, same arithmetic: bit-identical energy and forces
     assert e.item() == np.float32(ref["energy"].item())
     assert torch.equal(-g, ref["forces"])
+    # and the FP64 oracle on the same (FP32-rounded) coordinates, at the mixed tolerances:
+    # energy within 1e-6 of the summed term magnitudes, force RMS error < 1e-5
+    orc = oracle_water(wb, x.detach().double().cpu().numpy(), flexible=flexible)
+    assert abs(e.item() - orc["energy"]) < 1e-6 * orc["scale"]
+    assert rel_rms(-g, -orc["grad"]) < 1e-5
     e2, f2 = m.system.energy_forces(x.detach(), b)
     assert torch.equal(f2, ref["forces"])
     # saved, then run by a fresh process that only loads libtffb200_torch.so

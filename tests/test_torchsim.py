@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 import torch
 
-from gpu_util import rel, rel_max
+from gpu_util import oracle_water, rel, rel_max
 
 
 @dataclass
@@ -80,6 +80,10 @@ def test_single_system_matches_fixed_charge_system(flexible):
     assert out["energy"].shape == (1,) and out["forces"].shape == (wb.natoms, 3)
     assert rel(out["energy"][0] * TS.KJMOL_PER_EV, ref["energy"]) < 1e-12
     assert rel_max(out["forces"] * (TS.KJMOL_PER_EV / TS.NM_PER_ANGSTROM), ref["forces"]) < 1e-11
+    # the FP64 oracle in the reference's units: energy 1e-10 relative, forces 1e-8 of the largest
+    orc = oracle_water(wb, flexible=flexible)
+    assert rel(out["energy"][0] * TS.KJMOL_PER_EV, orc["energy"]) < 1e-10
+    assert rel_max(out["forces"] * (TS.KJMOL_PER_EV / TS.NM_PER_ANGSTROM), -orc["grad"]) < 1e-8
 
 
 @pytest.mark.gpu

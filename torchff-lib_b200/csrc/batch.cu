@@ -289,7 +289,7 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
   cluster_bounds_kernel<T><<<(int)std::max<int64_t>(1, std::min<int64_t>(nsup, 2 * sms)), kWarp * kSuper, 0, s>>>(cd);
   TFF_LAUNCHED();
   const int nb_cl = (int)std::max<int64_t>(1, std::min<int64_t>((ncl + 3) / 4, sms * 16));
-  cluster_neighbors_kernel<T><<<nb_cl, 128, 0, s>>>(cd, b->desc.cutoff, 0);
+  cluster_neighbors_kernel<T><<<nb_cl, 128, 0, s>>>(cd, b->desc.cutoff, /*half=*/1);
   TFF_LAUNCHED();
   auto *lj = reinterpret_cast<typename V2<T>::type *>(w + L.lj);
   int *exslot = reinterpret_cast<int *>(w + L.exslot);
@@ -313,9 +313,9 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
     A.kc = b->desc.coul_constant;
     A.energies = e_tile;
     const int64_t max_items = ncl * ((L.cap + kItemTiles - 1) / kItemTiles);
-    constexpr int NW = TileCfg<T>::NW;
+    constexpr int NW = kPairTileWarps;
     const int nbt = (int)std::max<int64_t>(1, std::min<int64_t>((max_items + NW - 1) / NW, (int64_t)sms * 48 / NW));
-    tile_kernel<T, 0, kTileMinBlocksBatch><<<nbt, NW * kWarp, 0, s>>>(A);
+    pair_tile_kernel<T, NW, PairTileOcc<T>::min_blocks><<<nbt, NW * kWarp, 0, s>>>(A);
     TFF_LAUNCHED();
   }
   TFF_CUDA(cudaStreamWaitEvent(s, b->join_ev, 0));

@@ -1,0 +1,494 @@
+// Real-space energy + forces over HALF cluster lists (each pair evaluated once).
+//
+// Work item: cluster I (32 atoms, 4 sub-clusters of 8 consecutive atoms along the Hilbert
+// curve) and up to kItemTiles clusters J <= I of its half neighbour list (entries k,
+// k + n, ...). Lane l = ti + 8 tj (ti = 0..7, tj = 0..3) owns the i atoms 8c + ti of I's
+// four sub-clusters c, in registers. For each J:
+//   - J's 32 atoms (moved to the periodic image the pair needs) and parameters are staged
+//     in per-warp shared memory;
+//   - the 16 sub-tiles (I sub-cluster ci, J sub-cluster cj) are screened by the distance
+//     between the two sub-clusters' bounding boxes, computed from the same positions with
+//     the same rounding steps as the pair distance, so that a screened-out sub-tile provably
+//     holds no pair within the cutoff;
+//   - for every J sub-cluster with an active sub-tile, lane (ti, tj) takes the two j atoms
+//     8cj + tj and 8cj + tj + 4 as one paired operand (FADD2/FMUL2/FFMA2 in FP32) against
+//     its i atom of each active sub-tile: 64 pairs per sub-tile, each evaluated once;
+//   - the j-side force and charge-gradient sums of the two j atoms are reduce-scattered
+//     over the 8 lanes that hold them (warp shuffles), and each of those lanes adds one of
+//     the 8 sums into the int64 fixed-point (FP32 mode) or FP64 accumulators.
+// The i-side sums stay in registers for the whole item and are reduce-scattered over the 4
+// lanes of each i atom at its end. Pairs within one cluster (J == I) count j < i; excluded
+// pairs are skipped through a per-J bit mask of each i atom's excluded partners, and their
+// Ewald exclusion correction -k q_i q_j erf(alpha r)/r (r <= rc) is evaluated in FP64 once
+// per excluded pair, by item 0 of the cluster that holds the pair's later slot.
+// Integer accumulation is order-independent, so FP32-mode results are bit-identical run to
+// run; energies are summed per lane in a fixed order and added once per item.
+#pragma once
+
+namespace tff {
+namespace {
+
+// Paired arithmetic on two values: FP32 pairs map onto the packed FP32 instructions of
+// sm_100a; FP64 pairs are two scalar operations.
+template <class T> struct P2T;
+template <> struct P2T<float> { using type = float2; };
+template <> struct P2T<double> { using type = D2; };
+
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 p_splat(float a) { return make_float2(a, a); }
+__device__ __forceinline__ D2 p_add(D2 a, D2 b) { return D2{a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ D2 p_mul(D2 a, D2 b) { return D2{a.x * b.x, a.y * b.y}; }
+__device__ __forceinline__ D2 p_fma(D2 a, D2 b, D2 c) { return D2{fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)}; }
+__device__ __forceinline__ D2 p_splat(double a) { return D2{a, a}; }
+
+// Per-warp staging: cluster J's positions (moved to the pair's image; padding slots far
+// away) with the charge in w and LJ parameters (sigma/2, sqrt eps); the same for cluster I
+// (padding far the other way), and I's four sub-cluster boxes (lo xyz, hi xyz).
+template <class T, int NW>
+struct PairTileSmem {
+  typename V4<T>::type pos[NW][kWarp];
+  typename V2<T>::type lj[NW][kWarp];
+  typename V4<T>::type ipos[NW][kWarp];
+  typename V2<T>::type ilj[NW][kWarp];
+  T ibox[NW][4][6];
+};
+
+// j-side sums of the two j atoms of a lane (paired): dE/dr / r * (r_i - r_j) summed over
+// the lane's i atoms (the j force is its negative) and the k-free charge gradient.
+template <class T> struct JSums { typename P2T<T>::type fx, fy, fz, dq; };
+
+// Two pairs (i; j0, j1): LJ + erfc-screened Coulomb. dx, dy, dz = r_i - r_j (paired), with
+// r2 = dx^2, then + dy^2, then + dz^2 by fused multiply-adds (the order box_gap2 repeats);
+// ok0 / ok1: the pair may contribute (valid, not excluded, counted by this side). Charge
+// gradients are accumulated k-free (times k when added).
+__device__ __forceinline__ void pair2_eval(float2 dx, float2 dy, float2 dz, bool ok0, bool ok1, float qi, float kqi,
+                                           float sgi, float epi, float2 qj, float2 sgj, float2 epj, float rc2,
+                                           float alpha, float two_a_rpi, float &fxi, float &fyi, float &fzi,
+                                           float &dqi, JSums<float> &js, float2 &te) {
+  const float2 one2 = p_splat(1.f), mone2 = p_splat(-1.f);
+  float2 r2 = p_mul(dx, dx);
+  r2 = p_fma(dy, dy, r2);
+  r2 = p_fma(dz, dz, r2);
+  // pairs outside the cutoff (or masked) get rinv = 0, which zeroes every term below
+  const float2 rinv = make_float2((ok0 && r2.x <= rc2) ? rsqrtf(r2.x) : 0.f, (ok1 && r2.y <= rc2) ? rsqrtf(r2.y) : 0.f);
+  const float2 rinv2 = p_mul(rinv, rinv);
+  const float2 u = p_mul(p_mul(r2, rinv), p_splat(alpha));
+  // erfc(u) exp(u^2) by Abramowitz & Stegun 7.1.26 (see erfc_exp_as)
+  const float2 den = p_fma(u, p_splat(0.3275911f), one2);
+  const float2 tt = make_float2(__fdividef(1.f, den.x), __fdividef(1.f, den.y));
+  float2 poly = p_fma(tt, p_splat(1.061405429f), p_splat(-1.453152027f));
+  poly = p_fma(tt, poly, p_splat(1.421413741f));
+  poly = p_fma(tt, poly, p_splat(-0.284496736f));
+  poly = p_fma(tt, poly, p_splat(0.254829592f));
+  poly = p_mul(tt, poly);
+  const float2 mu2 = p_mul(u, u);
+  const float2 ex = make_float2(__expf(-mu2.x), __expf(-mu2.y));
+  const float2 ec = p_mul(poly, ex);
+  const float2 ecr = p_mul(ec, rinv);  // erfc(u) / r
+  const float2 cq = p_mul(qj, ecr);    // E_coul / (k q_i)
+  const float2 g = p_fma(p_splat(two_a_rpi), p_mul(ex, rinv), p_mul(ec, rinv2));
+  float2 dedr = p_mul(p_mul(g, rinv), p_mul(qj, p_splat(-kqi)));  // (dE/dr) / r, Coulomb
+  const float2 sig = p_add(p_splat(sgi), sgj);
+  const float2 eps = p_mul(p_splat(epi), epj);
+  const float2 sr2 = p_mul(p_mul(sig, sig), rinv2);
+  const float2 sr6 = p_mul(p_mul(sr2, sr2), sr2);
+  const float2 es6 = p_mul(eps, sr6);
+  dedr = p_fma(p_mul(es6, p_splat(-24.f)), p_mul(p_fma(sr6, p_splat(2.f), mone2), rinv2), dedr);
+  fxi = fmaf(dedr.x, dx.x, fmaf(dedr.y, dx.y, fxi));
+  fyi = fmaf(dedr.x, dy.x, fmaf(dedr.y, dy.y, fyi));
+  fzi = fmaf(dedr.x, dz.x, fmaf(dedr.y, dz.y, fzi));
+  dqi += cq.x + cq.y;
+  js.fx = p_fma(dedr, dx, js.fx);
+  js.fy = p_fma(dedr, dy, js.fy);
+  js.fz = p_fma(dedr, dz, js.fz);
+  js.dq = p_fma(p_splat(qi), ecr, js.dq);
+  te = p_fma(cq, p_splat(kqi), te);
+  te = p_fma(p_mul(es6, p_splat(4.f)), p_add(sr6, mone2), te);
+}
+
+__device__ __forceinline__ void pair2_eval(D2 dx, D2 dy, D2 dz, bool ok0, bool ok1, double qi, double kqi, double sgi,
+                                           double epi, D2 qj, D2 sgj, D2 epj, double rc2, double alpha,
+                                           double two_a_rpi, double &fxi, double &fyi, double &fzi, double &dqi,
+                                           JSums<double> &js, D2 &te) {
+  const double ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
+  const double qq[2] = {qj.x, qj.y}, ss[2] = {sgj.x, sgj.y}, ee[2] = {epj.x, epj.y};
+  const bool ok[2] = {ok0, ok1};
+  double jfx[2], jfy[2], jfz[2], jdq[2], e[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    jfx[k] = jfy[k] = jfz[k] = jdq[k] = e[k] = 0.0;
+    double r2 = ddx[k] * ddx[k];
+    r2 = fma(ddy[k], ddy[k], r2);
+    r2 = fma(ddz[k], ddz[k], r2);
+    if (ok[k] && r2 <= rc2) {
+      const double rinv = rsqrt(r2);
+      const double rinv2 = rinv * rinv;
+      const double u = alpha * (r2 * rinv);
+      double ec, ex;
+      erfc_exp(u, ec, ex);
+      const double ecr = ec * rinv;
+      const double cq = qq[k] * ecr;
+      double dedr = -kqi * qq[k] * (ec * rinv2 + two_a_rpi * ex * rinv) * rinv;
+      const double sig = sgi + ss[k];
+      const double eps = epi * ee[k];
+      const double sr2 = sig * sig * rinv2;
+      const double sr6 = sr2 * sr2 * sr2;
+      dedr -= 24.0 * eps * sr6 * (2.0 * sr6 - 1.0) * rinv2;
+      fxi += dedr * ddx[k];
+      fyi += dedr * ddy[k];
+      fzi += dedr * ddz[k];
+      dqi += cq;
+      jfx[k] = dedr * ddx[k];
+      jfy[k] = dedr * ddy[k];
+      jfz[k] = dedr * ddz[k];
+      jdq[k] = qi * ecr;
+      e[k] = kqi * cq + 4.0 * eps * sr6 * (sr6 - 1.0);
+    }
+  }
+  js.fx = p_add(js.fx, D2{jfx[0], jfx[1]});
+  js.fy = p_add(js.fy, D2{jfy[0], jfy[1]});
+  js.fz = p_add(js.fz, D2{jfz[0], jfz[1]});
+  js.dq = p_add(js.dq, D2{jdq[0], jdq[1]});
+  te = p_add(te, D2{e[0], e[1]});
+}
+
+// Bounding box of each lane's 8-lane group (lanes 8c .. 8c+7 hold sub-cluster c), over
+// valid atoms only; lo > hi for a group without any.
+template <class T>
+__device__ __forceinline__ void subcluster_box(bool valid, T x, T y, T z, T lo[3], T hi[3]) {
+  const T big = sizeof(T) == 4 ? T(3e37) : T(1e300);
+  lo[0] = valid ? x : big;
+  lo[1] = valid ? y : big;
+  lo[2] = valid ? z : big;
+  hi[0] = valid ? x : -big;
+  hi[1] = valid ? y : -big;
+  hi[2] = valid ? z : -big;
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = min(lo[k], __shfl_xor_sync(kFull, lo[k], o));
+      hi[k] = max(hi[k], __shfl_xor_sync(kFull, hi[k], o));
+    }
+  }
+}
+
+// Squared gap between two boxes with the rounding steps of the pair distance: per axis
+// the difference of two coordinates (monotone in each), then x^2, fma y, fma z (monotone in
+// each magnitude), so every pair of atoms of the two boxes has r2 >= the result. Empty
+// boxes (lo > hi) give a huge gap.
+template <class T>
+__device__ __forceinline__ T box_gap2(const T alo[3], const T ahi[3], const T blo[3], const T bhi[3]) {
+  T g[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) g[k] = max(T(0), max(blo[k] - ahi[k], alo[k] - bhi[k]));
+  T r = g[0] * g[0];
+  r = fma(g[1], g[1], r);
+  r = fma(g[2], g[2], r);
+  return r;
+}
+
+// One halving step of a reduce-scatter over lanes that differ in lane bit `o`: a lane with
+// that bit set keeps the upper half of v[0, n), the other the lower half, each adding the
+// partner's copy of the half it keeps (stored in v[0, n/2)).
+template <class T, int N, int n>
+__device__ __forceinline__ void rs_halve(T (&v)[N], int o, int lane) {
+  const bool up = (lane & o) != 0;
+#pragma unroll
+  for (int q = 0; q < n / 2; ++q) {
+    const T keep = up ? v[q + n / 2] : v[q];
+    const T send = up ? v[q] : v[q + n / 2];
+    v[q] = keep + __shfl_xor_sync(kFull, send, o);
+  }
+}
+
+// Warps per block, and resident blocks per SM the register allocation must allow (FP32:
+// at most 80 registers; FP64 at most 128).
+constexpr int kPairTileWarps = 4;
+template <class T> struct PairTileOcc { static constexpr int min_blocks = sizeof(T) == 4 ? 5 : 3; };
+
+template <class T, int NW, int MIN_BLOCKS>
+__global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs<T> A) {
+  pdl_enter();
+  using V = typename V4<T>::type;
+  using W2 = typename V2<T>::type;
+  using P2 = typename P2T<T>::type;
+  __shared__ PairTileSmem<T, NW> sm;
+  __shared__ T s_box[NW][2][9];  // box and inverse of the warp's current system
+  const ClusterData<T> &cl = A.cl;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int ti = lane & 7, tj = lane >> 3;
+  T *s_m = s_box[w][0], *s_inv = s_box[w][1];
+  int cur_sys = -1;
+  bool ortho = false;
+  const T rc2 = (T)(A.rc * A.rc);
+  const T alpha = (T)A.alpha;
+  const T kc = (T)A.kc;
+  const T two_a_rpi = (T)(2.0 * A.alpha / 1.7724538509055160273);
+  const T far = sizeof(T) == 4 ? T(1e18) : T(1e150);  // padding slots: outside every cutoff
+
+  const int nitems = cl.itemoff[cl.nclusters];
+  const int nwarps = gridDim.x * NW;
+  for (int it = blockIdx.x * NW + w; it < nitems; it += nwarps) {
+    const int I = cl.items[it];  // owning cluster: itemoff[I] <= it < itemoff[I + 1]
+    const int isys = cl.system_of(I);
+    const double *info = cl.info(isys);
+    if (isys != cur_sys) {
+      __syncwarp();
+      if (lane < 9) {
+        s_m[lane] = (T)info[lane];
+        s_inv[lane] = (T)info[9 + lane];
+      }
+      ortho = info[18] != 0.0;
+      cur_sys = isys;
+      __syncwarp();
+    }
+    const int k = it - cl.itemoff[I];
+    const int nch = cl.itemoff[I + 1] - cl.itemoff[I];
+    const int cnt = cl.ncount[I];
+    const int ntile = (cnt - k + nch - 1) / nch;  // this item takes list entries k, k+nch, ...
+    const int64_t sI = (int64_t)I * kWarp;
+
+    // lane-as-atom view of I: staging (padding slots far away, never counted), sub-cluster
+    // boxes and the excluded-partner row. The lane's own i atoms are 8c + ti, c = 0..3.
+    const int64_t sl = sI + lane;
+    const bool vl = cl.sidx[sl] >= 0;
+    const unsigned ivalid = __ballot_sync(kFull, vl);
+    {
+      V p = cl.pos[sl];
+      T lo[3], hi[3];
+      subcluster_box<T>(vl, p.x, p.y, p.z, lo, hi);
+      if (!vl) p.x = p.y = p.z = -far;
+      __syncwarp();  // every lane is done with the previous item's staging
+      sm.ipos[w][lane] = p;
+      sm.ilj[w][lane] = A.lj[sl];
+      if (ti == 0) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          sm.ibox[w][tj][q] = lo[q];
+          sm.ibox[w][tj][3 + q] = hi[q];
+        }
+      }
+    }
+    const V ci = cl.bc[I], hi_ = cl.bh[I];
+    // every j atom moved to its image nearest I's centre is the minimum image of every
+    // in-cutoff pair when I's half extent + rc < L/2 on each axis (orthorhombic boxes)
+    const bool atom_shift = ortho && (hi_.x + (T)A.rc * s_inv[0] < T(0.499)) &&
+                            (hi_.y + (T)A.rc * s_inv[4] < T(0.499)) && (hi_.z + (T)A.rc * s_inv[8] < T(0.499));
+    const T cx = ci.x * s_m[0], cy = ci.y * s_m[4], cz = ci.z * s_m[8];
+    const int4 *xs_row = reinterpret_cast<const int4 *>(A.exslot + sl * kMaxExcl);
+    int x_lo, x_hi;  // the warp's range of clusters holding an excluded partner
+    {
+      const int4 a = xs_row[0], b = xs_row[1];
+      const int xs[kMaxExcl] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      int lo = 0x7fffffff, hi = -1;
+#pragma unroll
+      for (int x = 0; x < kMaxExcl; ++x)
+        if (xs[x] >= 0) {
+          lo = min(lo, xs[x] >> 5);
+          hi = max(hi, xs[x] >> 5);
+        }
+      x_lo = __reduce_min_sync(kFull, lo);
+      x_hi = __reduce_max_sync(kFull, hi);
+    }
+
+    T fx[4] = {T(0), T(0), T(0), T(0)}, fy[4] = {T(0), T(0), T(0), T(0)}, fz[4] = {T(0), T(0), T(0), T(0)};
+    T dq[4] = {T(0), T(0), T(0), T(0)};
+    double ep = 0.0;
+
+    for (int t = 0; t < ntile; ++t) {
+      const int J = cl.nbr[(int64_t)I * cl.cap + k + t * nch];
+      const int64_t sJ = (int64_t)J * kWarp;
+      // one periodic shift for the whole cluster pair when every pair's displacement then
+      // lies within half a box length per axis (orthorhombic boxes)
+      bool shifted = false;
+      T sx = T(0), sy = T(0), sz = T(0);
+      if (ortho && !atom_shift) {
+        const V cj = cl.bc[J], hj = cl.bh[J];
+        const T dcx = ci.x - cj.x, dcy = ci.y - cj.y, dcz = ci.z - cj.z;
+        const T nx = floor(dcx + T(0.5)), ny = floor(dcy + T(0.5)), nz = floor(dcz + T(0.5));
+        shifted = (fabs(dcx - nx) + hi_.x + hj.x < T(0.49)) && (fabs(dcy - ny) + hi_.y + hj.y < T(0.49)) &&
+                  (fabs(dcz - nz) + hi_.z + hj.z < T(0.49));
+        sx = nx * s_m[0];
+        sy = ny * s_m[4];
+        sz = nz * s_m[8];
+      }
+      const bool vj = cl.sidx[sJ + lane] >= 0;
+      V pj = cl.pos[sJ + lane];
+      if (atom_shift) {
+        pj.x += rint((cx - pj.x) * s_inv[0]) * s_m[0];
+        pj.y += rint((cy - pj.y) * s_inv[4]) * s_m[4];
+        pj.z += rint((cz - pj.z) * s_inv[8]) * s_m[8];
+        shifted = true;
+      } else if (shifted) {
+        pj.x += sx;
+        pj.y += sy;
+        pj.z += sz;
+      }
+      if (!vj) {
+        pj.x = far;
+        pj.y = far;
+        pj.z = far;
+        pj.w = T(0);
+      }
+      const unsigned jvalid = __ballot_sync(kFull, vj);
+      __syncwarp();  // every lane is done with the previous J's staging
+      sm.pos[w][lane] = pj;
+      sm.lj[w][lane] = A.lj[sJ + lane];
+      // active sub-tiles: bit ci + 4 cj. Without a common shift every sub-tile is taken.
+      unsigned act = 0xffffu;
+      if (shifted) {
+        T jlo[3], jhi[3];
+        subcluster_box<T>(vj, pj.x, pj.y, pj.z, jlo, jhi);
+        const int a = (lane & 3) * 8, b = ((lane >> 2) & 3) * 8;
+        T alo[3], ahi[3], blo[3], bhi[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          alo[q] = sm.ibox[w][a >> 3][q];
+          ahi[q] = sm.ibox[w][a >> 3][3 + q];
+          blo[q] = __shfl_sync(kFull, jlo[q], b);
+          bhi[q] = __shfl_sync(kFull, jhi[q], b);
+        }
+        act = __ballot_sync(kFull, lane < 16 && box_gap2<T>(alo, ahi, blo, bhi) <= rc2) & 0xffffu;
+      }
+      // pairs inside one cluster: j < i, i.e. only sub-tiles cj <= ci (per pair when equal)
+      const bool diag = J == I;
+      if (diag) act &= 0x8cefu;
+      // excluded-partner masks of this lane's i atoms over J's slots (bit = j index in J)
+      const bool special = diag || (J >= x_lo && J <= x_hi);
+      unsigned xm[4] = {0u, 0u, 0u, 0u};
+      if (special) {
+        const int4 a = xs_row[0], b = xs_row[1];
+        const int xs[kMaxExcl] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        unsigned m = 0u;
+#pragma unroll
+        for (int x = 0; x < kMaxExcl; ++x)
+          if (xs[x] >= 0 && (xs[x] >> 5) == J) m |= 1u << (xs[x] & 31);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) xm[c] = __shfl_sync(kFull, m, 8 * c + ti);
+      }
+      __syncwarp();
+      P2 te = p_splat(T(0));
+#pragma unroll 1
+      for (int cj = 0; cj < 4; ++cj) {
+        const unsigned col = (act >> (4 * cj)) & 0xfu;  // i sub-clusters active against cj
+        if (!col) continue;
+        const int j0 = 8 * cj + tj, j1 = j0 + 4;
+        const V a0 = sm.pos[w][j0], a1 = sm.pos[w][j1];
+        const W2 l0 = sm.lj[w][j0], l1 = sm.lj[w][j1];
+        const P2 nxj = P2{-a0.x, -a1.x}, nyj = P2{-a0.y, -a1.y}, nzj = P2{-a0.z, -a1.z};
+        const P2 qj = P2{a0.w, a1.w}, sgj = P2{l0.x, l1.x}, epj = P2{l0.y, l1.y};
+        const bool vj0 = (jvalid >> j0) & 1u, vj1 = (jvalid >> j1) & 1u;
+        JSums<T> js;
+        js.fx = js.fy = js.fz = js.dq = p_splat(T(0));
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (!((col >> c) & 1u)) continue;
+          const V pi = sm.ipos[w][8 * c + ti];
+          const W2 li = sm.ilj[w][8 * c + ti];
+          P2 dx = p_add(p_splat(pi.x), nxj);
+          P2 dy = p_add(p_splat(pi.y), nyj);
+          P2 dz = p_add(p_splat(pi.z), nzj);
+          const bool vi = (ivalid >> (8 * c + ti)) & 1u;
+          bool ok0 = vi, ok1 = vi;
+          if (!shifted) {
+            // per-pair minimum image; padding j atoms must be masked here (their far
+            // position does not survive the wrap)
+            pair_min_image(ortho, dx.x, dy.x, dz.x, s_m, s_inv);
+            pair_min_image(ortho, dx.y, dy.y, dz.y, s_m, s_inv);
+            ok0 = ok0 && vj0;
+            ok1 = ok1 && vj1;
+          }
+          if (special) {
+            const int il = 8 * c + ti;
+            ok0 = ok0 && !((xm[c] >> j0) & 1u) && (!diag || j0 < il);
+            ok1 = ok1 && !((xm[c] >> j1) & 1u) && (!diag || j1 < il);
+          }
+          pair2_eval(dx, dy, dz, ok0, ok1, pi.w, kc * pi.w, li.x, li.y, qj, sgj, epj, rc2, alpha, two_a_rpi,
+                     fx[c], fy[c], fz[c], dq[c], js, te);
+        }
+        // j side (dE/dx_j = -sum over i of (dE/dr)/r (r_i - r_j)): reduce-scatter over the 8
+        // lanes ti that hold j0, j1; lane ti ends with value ti (j0: x y z q, j1: x y z q)
+        T v[8] = {-js.fx.x, -js.fy.x, -js.fz.x, js.dq.x, -js.fx.y, -js.fy.y, -js.fz.y, js.dq.y};
+        rs_halve<T, 8, 8>(v, 4, lane);
+        rs_halve<T, 8, 4>(v, 2, lane);
+        rs_halve<T, 8, 2>(v, 1, lane);
+        const int64_t sj = sJ + (ti < 4 ? j0 : j1);
+        const int comp = ti & 3;
+        if ((jvalid >> (ti < 4 ? j0 : j1)) & 1u) {
+          if (comp < 3)
+            Acc<T>::add(&A.gx[3 * sj + comp], (double)v[0]);
+          else
+            Acc<T>::add(&A.gq[sj], (double)A.kc * (double)v[0]);
+        }
+      }
+      ep += (double)te.x + (double)te.y;
+    }
+    // i side: reduce-scatter over the 4 lanes tj of each i atom; lane tj ends with the four
+    // sums (x, y, z, q) of its atom c = tj
+    {
+      T v[16];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        v[4 * c] = fx[c];
+        v[4 * c + 1] = fy[c];
+        v[4 * c + 2] = fz[c];
+        v[4 * c + 3] = dq[c];
+      }
+      rs_halve<T, 16, 16>(v, 16, lane);
+      rs_halve<T, 16, 8>(v, 8, lane);
+      if (vl) {  // atom 8 tj + ti is this lane's own slot sl
+        Acc<T>::add(&A.gx[3 * sl], (double)v[0]);
+        Acc<T>::add(&A.gx[3 * sl + 1], (double)v[1]);
+        Acc<T>::add(&A.gx[3 * sl + 2], (double)v[2]);
+        Acc<T>::add(&A.gq[sl], (double)A.kc * (double)v[3]);
+      }
+    }
+    ep = warp_sum(ep);
+
+    // Ewald exclusion correction, FP64, once per excluded pair (by the later slot's cluster,
+    // item 0): -k q_i q_p erf(alpha r)/r for r <= rc, minimum image of the box
+    double ex = 0.0;
+    if (k == 0) {
+      const double *m = info, *inv = info + 9;
+      const double kcd = A.kc, ad = A.alpha, ta = 2.0 * A.alpha / 1.7724538509055160273;
+      const int4 a = xs_row[0], b = xs_row[1];
+      const int xs[kMaxExcl] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      const V pl = cl.pos[sl];
+#pragma unroll 1
+      for (int x = 0; x < kMaxExcl; ++x) {
+        const int p = xs[x];
+        if (!vl || p < 0 || p >= sl) continue;
+        const V pp = cl.pos[p];
+        double dx = (double)pl.x - (double)pp.x, dy = (double)pl.y - (double)pp.y, dz = (double)pl.z - (double)pp.z;
+        min_image(dx, dy, dz, m, inv);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 <= A.rc * A.rc) || r2 == 0.0) continue;
+        const double rinv = rsqrt(r2), r = r2 * rinv;
+        const double damp = -erf(ad * r);
+        const double e2 = exp(-ad * ad * r2);
+        const double kq = kcd * (double)pl.w * (double)pp.w;
+        const double dedr = -kq * (damp * rinv * rinv + ta * e2 * rinv) * rinv;
+        ex += kq * damp * rinv;
+        Acc<T>::add(&A.gx[3 * sl], dedr * dx);
+        Acc<T>::add(&A.gx[3 * sl + 1], dedr * dy);
+        Acc<T>::add(&A.gx[3 * sl + 2], dedr * dz);
+        Acc<T>::add(&A.gx[3 * (int64_t)p], -dedr * dx);
+        Acc<T>::add(&A.gx[3 * (int64_t)p + 1], -dedr * dy);
+        Acc<T>::add(&A.gx[3 * (int64_t)p + 2], -dedr * dz);
+        Acc<T>::add(&A.gq[sl], kcd * (double)pp.w * damp * rinv);
+        Acc<T>::add(&A.gq[p], kcd * (double)pl.w * damp * rinv);
+      }
+      ex = warp_sum(ex);
+    }
+    if (lane == 0) {
+      Acc<T>::add(&A.energies[2 * isys], ep);
+      if (k == 0) Acc<T>::add(&A.energies[2 * isys + 1], ex);
+    }
+  }
+}
+
+}  // namespace
+}  // namespace tff

@@ -121,10 +121,8 @@ __device__ __forceinline__ void pair_min_image(bool ortho, T &dx, T &dy, T &dz, 
 }
 
 // Resident 4-warp blocks per SM the register allocation of the energy kernel must allow
-// (6 blocks = 24 warps: at most 80 registers per thread). The batched evaluation, whose
-// many small systems leave more work items in flight, runs best at 7 (at most 73).
+// (6 blocks = 24 warps: at most 80 registers per thread).
 constexpr int kTileMinBlocks = 6;
-constexpr int kTileMinBlocksBatch = 7;
 
 template <class T, int MODE = 0, int MIN_BLOCKS = kTileMinBlocks>
 __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? MIN_BLOCKS : 1)
@@ -693,3 +691,5 @@ inline std::vector<double> host_moduli(int K, int count) {
 
 }  // namespace
 }  // namespace tff
+
+#include "pair_tile.cuh"
