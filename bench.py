@@ -163,7 +163,7 @@ def measured_peaks() -> dict:
         return {}
 
 
-PROFILED_SOURCES = ("tile.cuh", "cluster.cuh", "tff_common.cuh", "fused.cu")
+PROFILED_SOURCES = ("pair_tile.cuh", "tile.cuh", "cluster.cuh", "tff_common.cuh", "fused.cu")
 
 
 def kernel_source_hash() -> str:
@@ -653,8 +653,8 @@ def run_ours(args):
         flops = 60.0 * npairs                                   # algorithmic flops per launch
         achieved = flops / (tile_mean_ms * 1e-3) / 1e12
         stages = {k: round(v / n_stage * 1e3, 3) for k, v in stage_acc.items()}
-        traffic = ncu_traffic("tile_kernel", args.workload)
-        issue = ncu_traffic("tile_kernel", args.workload, "ncu_issue.txt")
+        traffic = ncu_traffic("pair_tile_kernel", args.workload)
+        issue = ncu_traffic("pair_tile_kernel", args.workload, "ncu_issue.txt")
         result = {
             "metric": METRIC if args.workload == "water3000" else f"{args.workload} PME energy+force evals/s",
             "value": round(value, 2),
@@ -683,7 +683,7 @@ def run_ours(args):
                     "path": "tff_system_eval_host (C ABI): pinned host coords/box -> device -> host forces"},
             "gpu_launches": system.kernel_launches() * args.steps,
             "roofline": {
-                "kernel": "tile_kernel<float> (fused real-space LJ + erfc Coulomb, 32x32 cluster tiles)",
+                "kernel": "pair_tile_kernel<float> (fused real-space LJ + erfc Coulomb over half cluster lists, 8x8 sub-tiles, each pair once)",
                 "bound": "fp32",
                 "achieved": round(achieved, 4),
                 "peak": round(fp32_peak, 2),
@@ -697,9 +697,9 @@ def run_ours(args):
                                "MEASURED_PEAKS.json; no measured FP32 peak exists)",
                 "issue_active": issue["value"],
                 "issue_source": issue,
-                "issue_note": "the tile kernel is bound by instruction issue (mask building, bit walk, "
-                              "pair math), not by the FP32 pipe: fraction of issue slots used, from ncu "
-                              "(profiles/ncu_issue.txt)",
+                "issue_note": "fraction of issue slots the pair kernel uses, from ncu (profiles/ncu_issue.txt): "
+                              "sub-tile screening, staging and the shuffle reductions share the issue slots "
+                              "with the pair math",
             },
         }
         result["throughput"] = throughput_fields(npairs, value, tile_mean_ms, traffic["value"])
@@ -797,7 +797,8 @@ def import_reference_cpu():
     baseline/_ref) imported for its pure-torch path. Its modules import their compiled
     extension modules by name; the pure-torch path never calls them, so empty modules stand
     in. torchff/pme_ref.py:8 switches the default device to CUDA at import time; it is set
-    back to the CPU afterwards. Returns None when the install is absent."""
+    back to the CPU afterwards, and the default dtype to FP64. Returns None when the install
+    is absent."""
     import types
 
     root = os.path.join(REPO, "baseline", "_ref")
@@ -815,6 +816,10 @@ def import_reference_cpu():
     from torchff.vdw import Vdw
 
     torch.set_default_device("cpu")
+    # FP64 throughout: the pure-torch PME builds its B-spline moduli from default-dtype
+    # tensors (torchff/pme_ref.py:268-274), which FP32 would round to ~1e-6 of the
+    # reciprocal energy
+    torch.set_default_dtype(torch.float64)
     return types.SimpleNamespace(NeighborList=NeighborList, MultipolarInteraction=MultipolarInteraction, PME=PME,
                                  Vdw=Vdw, root=root)
 

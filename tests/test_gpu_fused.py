@@ -370,11 +370,21 @@ def test_large_box_matches_independent_composition():
 
 def test_water100k_against_oracle():
     """The 100,000-water box (300,000 atoms, L = 14.42 nm, rc = 1.0 nm, PME 144^3): FP64
-    total energy against the oracle (cell-binned real space + PME) to 1e-10 relative, FP64
+    total energy against the oracle (cell-binned real space + PME) to 1e-12 of the summed
+    magnitudes of the real-space and reciprocal terms (each about 2.1e7 kJ/mol; their sum,
+    3.1e4, cancels 690-fold, so this is about 7e-10 of the total: FP64 sums over 63 M pairs
+    in different orders, here and in the oracle, agree to a few 1e-13 of the terms), FP64
     forces on 256 sampled atoms against the oracle (distances to every atom + PME gathered
-    there) to 1e-8 of their largest component, mixed precision against FP64: force RMS
-    error < 1e-5 and energy within 1e-6 of the summed term magnitudes; both status words 0
-    (no cluster list cut at this size)."""
+    there) to 1e-8 of their largest component; both status words 0 (no cluster list cut at
+    this size).
+
+    Mixed precision: its arithmetic against FP64 evaluated at the same (FP32) coordinates,
+    force RMS error < 1e-5 and energy within 1e-6 of the summed term magnitudes; and the
+    whole error against FP64 at the original coordinates < 2e-5. The second bound is wider
+    because rounding the inputs to FP32 moves atoms by up to 4.8e-7 nm in the outer half of
+    a 14.42 nm box (FP32 spacing 9.5e-7 nm between 8 and 16), which alone changes the
+    FP64 forces by about 1e-5 RMS (at 3000 waters, L = 4.48 nm, the same rounding gives
+    4.0e-6 of the mixed path's 4.5e-6)."""
     from torchff_b200.system import FixedChargeSystem
     from torchff_b200.water import water_box_100k
 
@@ -382,20 +392,23 @@ def test_water100k_against_oracle():
     s64 = FixedChargeSystem.from_water_box(wb, dtype=torch.float64)
     o64 = s64.evaluate(t(wb.coords), t(wb.box), terms=True)
     assert s64.status() == 0
+    x32, b32 = t(wb.coords, torch.float32), t(wb.box, torch.float32)
+    o64r = s64.evaluate(x32.double(), b32.double(), terms=True)
     s32 = FixedChargeSystem.from_water_box(wb, dtype=torch.float32)
-    o32 = s32.evaluate(t(wb.coords, torch.float32), t(wb.box, torch.float32))
+    o32 = s32.evaluate(x32, b32)
     assert s32.status() == 0
     f64 = o64["forces"].cpu().numpy()
-    assert rel_rms(o32["forces"], f64) < 1e-5
-    scale = float(o64["terms"].abs().sum())
-    assert abs(o32["energy"].item() - o64["energy"].item()) < 1e-6 * scale
+    assert rel_rms(o32["forces"], o64r["forces"].cpu().numpy()) < 1e-5
+    assert rel_rms(o32["forces"], f64) < 2e-5
+    scale = float(o64r["terms"].abs().sum())
+    assert abs(o32["energy"].item() - o64r["energy"].item()) < 1e-6 * scale
 
     k = 138.935456
     e_real = O.real_space_cells(wb.coords, wb.box, wb.charges, wb.atom_types, wb.sigma_table, wb.epsilon_table,
                                 wb.coulomb_exclusions, wb.cutoff, wb.alpha, k)
     subset = np.random.default_rng(11).choice(wb.natoms, 256, replace=False)
     e_pme, g_pme = O.pme_subset(wb.coords, wb.box, wb.charges, wb.alpha, wb.grid, subset)
-    assert rel(o64["energy"].item(), e_real + k * e_pme) < 1e-10
+    assert abs(o64["energy"].item() - (e_real + k * e_pme)) < 1e-12 * (abs(e_real) + abs(k * e_pme))
     g = O.real_space_grad_subset(wb.coords, wb.box, wb.charges, wb.atom_types, wb.sigma_table, wb.epsilon_table,
                                  wb.coulomb_exclusions, wb.cutoff, wb.alpha, k, subset) + k * g_pme
     assert np.max(np.abs(-f64[subset] - g)) < 1e-8 * np.max(np.abs(g))

@@ -289,7 +289,7 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
   cluster_bounds_kernel<T><<<(int)std::max<int64_t>(1, std::min<int64_t>(nsup, 2 * sms)), kWarp * kSuper, 0, s>>>(cd);
   TFF_LAUNCHED();
   const int nb_cl = (int)std::max<int64_t>(1, std::min<int64_t>((ncl + 3) / 4, sms * 16));
-  cluster_neighbors_kernel<T><<<nb_cl, 128, 0, s>>>(cd, b->desc.cutoff, /*half=*/1);
+  cluster_neighbors_kernel<T><<<nb_cl, 128, 0, s>>>(cd, b->desc.cutoff, kHalfLists<T>);
   TFF_LAUNCHED();
   auto *lj = reinterpret_cast<typename V2<T>::type *>(w + L.lj);
   int *exslot = reinterpret_cast<int *>(w + L.exslot);
@@ -313,10 +313,8 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
     A.kc = b->desc.coul_constant;
     A.energies = e_tile;
     const int64_t max_items = ncl * ((L.cap + kItemTiles - 1) / kItemTiles);
-    constexpr int NW = kPairTileWarps;
-    const int nbt = (int)std::max<int64_t>(1, std::min<int64_t>((max_items + NW - 1) / NW, (int64_t)sms * 48 / NW));
-    pair_tile_kernel<T, NW, PairTileOcc<T>::min_blocks><<<nbt, NW * kWarp, 0, s>>>(A);
-    TFF_LAUNCHED();
+    const int st_rs = launch_real_space<T>(false, max_items, sms, s, A);
+    if (st_rs != TFF_OK) return st_rs;
   }
   TFF_CUDA(cudaStreamWaitEvent(s, b->join_ev, 0));
   const int nbf = (int)std::max<int64_t>(1, std::min<int64_t>((total_atoms + 255) / 256, sms * 8));

@@ -134,9 +134,8 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
   // the real-space chain (cluster build, sorted parameters, tile kernel) is one run of
   // programmatic dependent launches unless stage events sit between its kernels
   const bool pdl = ev == nullptr;
-  // half lists (J <= I): the pair kernel evaluates every pair once
   st = build_clusters<T>(sys->cl, cd, sys->cl_ws, x, static_cast<const T *>(sys->q), box, sys->desc.cutoff,
-                         /*half=*/1, s, sys->scratch, 8 * sizeof(double), pdl);
+                         kHalfLists<T>, s, sys->scratch, 8 * sizeof(double), pdl);
   if (st != TFF_OK) return st;
   if ((st = mark(1, s)) != TFF_OK) return st;
   if (use_pme) {
@@ -174,10 +173,7 @@ int system_eval_impl(tff_system sys, const T *x, const T *box, double *energy, T
     // work items are only known on the device: size the grid for the largest possible
     // count (every cluster with a full list), capped at a few waves of the SMs
     const int64_t max_items = sys->cl.nclusters * ((sys->cl.cap + kItemTiles - 1) / kItemTiles);
-    constexpr int NW = kPairTileWarps;
-    const int nbt = (int)std::max<int64_t>(1, std::min<int64_t>((max_items + NW - 1) / NW, (int64_t)sms * 48 / NW));
-    if ((st = launch_k(pdl, pair_tile_kernel<T, NW, PairTileOcc<T>::min_blocks>, nbt, NW * kWarp, 0, s, A)) != TFF_OK)
-      return st;
+    if ((st = launch_real_space<T>(pdl, max_items, sms, s, A)) != TFF_OK) return st;
   }
   if ((st = mark(2, s)) != TFF_OK) return st;
   if (use_pme) TFF_CUDA(cudaStreamWaitEvent(s, sys->join_ev, 0));
