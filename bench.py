@@ -934,10 +934,12 @@ def run_reference_gpu(args):
                            "(rank 0, pairs_excl) + 138.935456 x pme_long_range, energy + backward",
                    "timing": f"{r['fp64_timing_mode']}, {r['l2']}"},
         "fp64": {"evals_per_s": round(r["fp64_evals_per_s"], 2), "ms_per_eval": round(r["fp64_ms_per_eval"], 5),
-                 "mode": r["fp64_timing_mode"], "energy_rel_err_vs_oracle": r.get("fp64_energy_rel_err_vs_oracle"),
+                 "mode": r["fp64_timing_mode"], "capture_error": r.get("fp64_capture_error"),
+                 "energy_rel_err_vs_oracle": r.get("fp64_energy_rel_err_vs_oracle"),
                  "force_rel_rms_vs_oracle": r.get("fp64_force_rel_rms_vs_oracle")},
         "fp32": {"evals_per_s": round(r["fp32_evals_per_s"], 2), "ms_per_eval": round(r["fp32_ms_per_eval"], 5),
-                 "mode": r["fp32_timing_mode"], "energy_rel_err_vs_oracle": r.get("fp32_energy_rel_err_vs_oracle"),
+                 "mode": r["fp32_timing_mode"], "capture_error": r.get("fp32_capture_error"),
+                 "energy_rel_err_vs_oracle": r.get("fp32_energy_rel_err_vs_oracle"),
                  "force_rel_rms_vs_oracle": r.get("fp32_force_rel_rms_vs_oracle")},
         "clocks": clocks.summary(),
     }

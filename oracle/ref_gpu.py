@@ -102,10 +102,11 @@ def energy(wb, d):
     return e_lj + e_c + e_p
 
 
-def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tuple[float, str]:
+def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tuple[float, str, str]:
     """ms per forward + backward: CUDA-graph replay as in torchff/test_utils.py:52-146, or,
     when the composition cannot be captured, eager calls. With flush_l2 a 256 MiB device
-    write (larger than the 126 MB L2) runs before every timed replay, outside its events."""
+    write (larger than the 126 MB L2) runs before every timed replay, outside its events.
+    Returns (ms, mode, the capture error when the mode is eager)."""
     import torch
 
     x = d["coords"]
@@ -120,6 +121,7 @@ def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tup
     flush = torch.empty(256 * 1024 * 1024 if flush_l2 else 1, dtype=torch.uint8, device="cuda")
     a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     mode = "cuda_graph"
+    error = ""
     total = 0.0
     try:
         g = torch.cuda.CUDAGraph()
@@ -131,8 +133,9 @@ def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tup
             g.replay()
         torch.cuda.synchronize()
         run = g.replay
-    except Exception:  # capture invalidated by a host synchronisation inside an op
+    except Exception as exc:  # capture invalidated by a host synchronisation inside an op
         mode = "eager"
+        error = f"{type(exc).__name__}: {str(exc).strip().splitlines()[0][:300] if str(exc).strip() else ''}"
         torch.cuda.synchronize()
 
         def run():
@@ -145,7 +148,7 @@ def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tup
         z.record()
         z.synchronize()
         total += a.elapsed_time(z)
-    return total / steps, mode
+    return total / steps, mode, error
 
 
 def measure(workload: str = "water3000", steps: int = 200, warmup: int = 5, check: bool = True,
@@ -167,8 +170,10 @@ def measure(workload: str = "water3000", steps: int = 200, warmup: int = 5, chec
         e.backward()
         out[f"{name}_energy"] = float(e.item())
         forces[name] = (-d["coords"].grad).double().cpu().numpy()
-        ms, mode = time_graph(wb, d, steps, warmup, flush_l2)
+        ms, mode, error = time_graph(wb, d, steps, warmup, flush_l2)
         out[f"{name}_ms_per_eval"], out[f"{name}_timing_mode"] = ms, mode
+        if error:
+            out[f"{name}_capture_error"] = error
         out[f"{name}_evals_per_s"] = 1e3 / ms
     if check:
         from oracle import oracle as O
