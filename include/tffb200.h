@@ -18,7 +18,8 @@
  *     matching *_workspace_bytes() reports; the library itself never calls cudaMalloc in
  *     these entry points (PME plans and system objects own their memory, see below).
  *   - Work is enqueued on `stream` (a cudaStream_t); nothing synchronises with the host
- *     except the *_host entry points. Every call can be captured in a CUDA graph.
+ *     except the *_host entry points. Calls of the entry points that take a workspace can
+ *     be captured in a CUDA graph.
  *   - Return value: TFF_OK or an error code; tff_last_error() describes the last error
  *     of the calling thread.
  */
