@@ -437,13 +437,21 @@ int tff_batch_destroy(tff_batch batch);
  * caller order: coords (sum natoms, 3), boxes (nsys, 3, 3), charges / sigma / epsilon
  * (sum natoms), excl (sum natoms, 8) int32 excluded partners as atom indices within
  * their own system, -1 padded; out: energies (nsys) float64, forces (sum natoms, 3) in the batch dtype.
- * The host part (system table, FFT grouping) runs in the call; the call returns once the
- * work is enqueued. One evaluation at a time per batch object and stream. */
+ * The host part (system table, work-unit offsets) runs in the call; the call returns once
+ * the work is enqueued. One evaluation at a time per batch object and stream.
+ * Every launch shape of the device part depends on the batch's capacity and the DFT size
+ * class (grid sides up to 52, or larger) alone; the composition is uploaded with the
+ * system table. So when a call repeats the previous call's device pointers and DFT class,
+ * the device part is captured in a CUDA graph, and later calls with those pointers and
+ * that class replay it whatever systems they hold (up to 8 graphs per batch object). */
 int tff_batch_eval(tff_batch batch, int nsys, const int64_t *natoms, const int *pme_grid, const void *coords,
                    const void *boxes, const void *charges, const void *sigma, const void *epsilon,
                    const int *excl, double *energies, void *forces, tff_stream_t stream);
 int tff_batch_status(tff_batch batch, tff_stream_t stream, int *status);
 int tff_batch_kernel_launches(tff_batch batch);
+/* No counterpart in the reference. Evaluations of this batch object so far that ran as a
+ * replay of a captured graph. */
+int64_t tff_batch_graph_launches(tff_batch batch);
 
 /* ------------------------------------------------------------------------------
  * Server: continuous batching of requests over tff_batch (no reference counterpart)

@@ -203,3 +203,74 @@ def test_batch_triclinic_system_matches_oracle():
                                     138.935456)
         assert rel(e[k].item(), ref["total"]) < 1e-10, k
         assert rel_max(f[k], -ref["grad_coords"]) < 1e-8, k
+
+
+def test_graph_replay_serves_other_compositions():
+    """Evaluations through one set of device buffers: the second call with the same buffers
+    and DFT size class captures the device part in a CUDA graph, and later calls of that
+    class replay it with other systems in the buffers. Every result is bit-identical to a
+    direct evaluation of the same systems by another batch object, and a class whose graph
+    is not yet captured runs directly."""
+    from torchff_b200.serving import BatchEvaluator, exclusion_table
+
+    # grid sides: a and c at most 30 (DFT class 52), b 54 (5,000 waters; the larger class)
+    sizes = {"a": [64, 900, 333], "b": [5000, 150], "c": [333, 64, 900, 150]}
+    boxes = {k: _boxes(v, seed0=40 + 10 * i) for i, (k, v) in enumerate(sizes.items())}
+    cap_atoms, cap_sys = 30_000, 8
+    wbs0 = boxes["a"][0]
+    ev = BatchEvaluator(RC, wbs0[0].alpha, torch.float32, max_systems=cap_sys, max_atoms=cap_atoms,
+                        max_grid_points=2_000_000)
+    ref_ev = BatchEvaluator(RC, wbs0[0].alpha, torch.float32, max_systems=cap_sys, max_atoms=cap_atoms,
+                            max_grid_points=2_000_000)
+    dev, f32 = torch.device("cuda"), torch.float32
+    buf = {"coords": torch.empty(3 * cap_atoms, dtype=f32, device=dev),
+           "boxes": torch.empty(9 * cap_sys, dtype=f32, device=dev),
+           "charges": torch.empty(cap_atoms, dtype=f32, device=dev),
+           "sigma": torch.empty(cap_atoms, dtype=f32, device=dev),
+           "epsilon": torch.empty(cap_atoms, dtype=f32, device=dev),
+           "excl": torch.empty(8 * cap_atoms, dtype=torch.int32, device=dev),
+           "energies": torch.empty(cap_sys, dtype=torch.float64, device=dev),
+           "forces": torch.empty(3 * cap_atoms, dtype=f32, device=dev)}
+
+    def packed_in_buffers(specs):
+        natoms = np.array([s.natoms for s in specs], dtype=np.int64)
+        n = int(natoms.sum())
+        cat = lambda a: torch.from_numpy(np.concatenate(a)).to(dev, f32)  # noqa: E731
+        buf["coords"][:3 * n] = cat([s.coords.reshape(-1) for s in specs])
+        buf["boxes"][:9 * len(specs)] = cat([s.box.reshape(-1) for s in specs])
+        buf["charges"][:n] = cat([s.charges for s in specs])
+        buf["sigma"][:n] = cat([s.sigma for s in specs])
+        buf["epsilon"][:n] = cat([s.epsilon for s in specs])
+        ex = np.concatenate([exclusion_table(s.natoms, s.excl_pairs) for s in specs]).reshape(-1)
+        buf["excl"][:ex.size] = torch.from_numpy(ex).to(dev)
+        return {"natoms": natoms, "pme_grid": np.array([s.pme_grid for s in specs], dtype=np.int32),
+                "coords": buf["coords"], "boxes": buf["boxes"], "charges": buf["charges"], "sigma": buf["sigma"],
+                "epsilon": buf["epsilon"], "excl": buf["excl"], "energies": buf["energies"],
+                "forces": buf["forces"]}, n
+
+    kept = []  # reference packs stay allocated, so each reference call has new addresses
+
+    def check(name):
+        specs = boxes[name][1]
+        p, n = packed_in_buffers(specs)
+        ev.evaluate_packed(p)
+        e = p["energies"][:len(specs)].clone()
+        f = p["forces"][:3 * n].clone()
+        kept.append(ref_ev.pack(specs))
+        ref_ev.evaluate_packed(kept[-1])  # always the direct path
+        torch.cuda.synchronize()
+        assert ev.status() == 0 and ref_ev.status() == 0
+        assert torch.equal(e, kept[-1]["energies"]), name
+        assert torch.equal(f, kept[-1]["forces"].reshape(-1)), name
+
+    check("a")                        # direct
+    check("a")                        # same buffers and class: captured, then replayed
+    assert ev.graph_launches() == 1
+    check("c")                        # the class-52 graph replayed with other systems
+    assert ev.graph_launches() == 2
+    check("b")                        # the larger class: direct
+    assert ev.graph_launches() == 2
+    check("b")                        # captured
+    check("a")                        # the class-52 graph again
+    assert ev.graph_launches() == 4
+    assert ref_ev.graph_launches() == 0

@@ -15,6 +15,7 @@
 // pass for all grid sizes): cuFFT transforms grids of one size per plan, and a batch of
 // a few hundred sizes would need hundreds of plans and launches per evaluation.
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <utility>
 #include <vector>
@@ -40,10 +41,14 @@ inline int moduli_offset(int K) {
   return off;
 }
 
+// Bytes before the system table in the uploaded block (the BatchShape sits there).
+constexpr size_t kTableOffset = 256;
+static_assert(sizeof(BatchShape) <= kTableOffset, "BatchShape must fit before the system table");
+
 struct BatchLayout {
   int64_t atoms, systems, clusters, supers, grid;
   int cap;
-  size_t sys, status, boxinfo, cl_sys, sup_sys, sidx, inv, pos, frac, bc, bh, sbc, sbh, nbr, ncount, itemoff, items;
+  size_t shape, sys, status, boxinfo, cl_sys, sup_sys, sidx, inv, pos, frac, bc, bh, sbc, sbh, nbr, ncount, itemoff, items;
   size_t lj, exslot, acc, e_tile;
   size_t fix, real, cplx, partials, tickets, e_pme, pme_grad, pme_phi, moduli;
   size_t bytes;
@@ -64,7 +69,9 @@ inline BatchLayout batch_layout(int dtype, int64_t max_atoms, int64_t max_system
     c.take<char>(bytes);
     return c.off - bytes;
   };
-  L.sys = take(max_systems * sizeof(BatchSys));
+  // shape and system table: one upload per evaluation (shape first, the table 256 bytes on)
+  L.shape = take(kTableOffset + max_systems * sizeof(BatchSys));
+  L.sys = L.shape + kTableOffset;
   L.status = take(64 * sizeof(unsigned));
   L.boxinfo = take(max_systems * kInfoStride * sizeof(double));
   L.cl_sys = take(L.clusters * sizeof(int));
@@ -104,17 +111,38 @@ inline BatchLayout batch_layout(int dtype, int64_t max_atoms, int64_t max_system
 
 using namespace tff;
 
+// Device pointers of one evaluation and the DFT size class: a captured graph replays only
+// for the same key.
+struct BatchGraphKey {
+  const void *ptr[10];
+  int dft_class;
+  bool operator==(const BatchGraphKey &o) const {
+    if (dft_class != o.dft_class) return false;
+    for (int k = 0; k < 10; ++k)
+      if (ptr[k] != o.ptr[k]) return false;
+    return true;
+  }
+};
+
 struct tff_batch_s {
   tff_batch_desc desc;
   BatchLayout L;
   char *ws = nullptr;
-  BatchSys *table = nullptr;       // pinned host copy of the system table
+  unsigned char *table = nullptr;  // pinned host copy of the shape + system table block
   cudaEvent_t table_ev = nullptr;  // the table upload of the previous evaluation
   cudaStream_t pme_stream = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   cudaEvent_t sorted_ev = nullptr;  // batch sort done (the PME gather visits its atom order)
   std::vector<BatchSys> host_sys;
   int device = 0;
+  // CUDA graphs of the evaluation (launch shapes depend on the capacity alone, the batch's
+  // composition is read from the uploaded shape): captured when a call repeats the
+  // previous call's key, replayed for every later call with that key
+  cudaStream_t capture_stream = nullptr;
+  std::vector<std::pair<BatchGraphKey, cudaGraphExec_t>> graphs;
+  BatchGraphKey last_key{};
+  bool have_last = false;
+  int64_t graph_launches = 0;
 };
 
 namespace tff {
@@ -122,6 +150,8 @@ namespace {
 
 void free_batch(tff_batch b) {
   if (!b) return;
+  for (auto &g : b->graphs) cudaGraphExecDestroy(g.second);
+  if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
   if (b->ws) cudaFree(b->ws);
   if (b->table) cudaFreeHost(b->table);
   if (b->table_ev) cudaEventDestroy(b->table_ev);
@@ -132,40 +162,23 @@ void free_batch(tff_batch b) {
   delete b;
 }
 
-// One direction of the 3-D real DFT of every grid of the batch (three axis passes).
-template <class T>
-int run_dft(const BatchSys *dsys, int nsys, int kmax, bool forward, T *real, typename CplxOf<T>::type *cplx,
-            cudaStream_t s) {
-  const dim3 grid((unsigned)kmax, (unsigned)nsys);
-  const size_t smem = batch_dft_smem<T>(kmax);
-  if (forward) {
-    batch_dft_kernel<T, kDftZR2C><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
-    TFF_LAUNCHED();
-    batch_dft_kernel<T, kDftY><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
-    TFF_LAUNCHED();
-    batch_dft_kernel<T, kDftX><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
-    TFF_LAUNCHED();
-  } else {
-    batch_dft_kernel<T, kDftXInv><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
-    TFF_LAUNCHED();
-    batch_dft_kernel<T, kDftYInv><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
-    TFF_LAUNCHED();
-    batch_dft_kernel<T, kDftZC2R><<<grid, kDftThreads, smem, s>>>(dsys, real, cplx);
-    TFF_LAUNCHED();
-  }
-  return TFF_OK;
-}
+// DFT shared-memory size class of a batch, part of the graph key: 52 for grid sides up to
+// 52 (every water box up to 4,000 waters at 0.1 nm spacing), else the dtype's limit. A
+// class costs a capture per lane, and the shared memory of the class sets the resident DFT
+// blocks: 5 per SM at 52 (FP32), where a 56 class gave 4 (25 % slower passes) and 64 gave 3.
+constexpr int kDftSmallClass = 52;
+inline int dft_class(int kmax, int kcap) { return kmax <= kDftSmallClass ? std::min(kcap, kDftSmallClass) : kcap; }
 
+// Host part of an evaluation: system table (offsets, cell grids, PME and DFT work units)
+// and shape into the pinned block, after the previous upload out of it is done. Returns
+// the table's largest grid side in *kmax.
 template <class T>
-int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme_grid, const T *x, const T *boxes,
-                    const T *q, const T *sigma, const T *eps, const int *excl, double *energies, T *forces,
-                    cudaStream_t s) {
-  using S = typename Acc<T>::S;
+int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_grid, int *kmax_out) {
   const BatchLayout &L = b->L;
-  // --- host: system table, grid order, FFT groups
   auto &hs = b->host_sys;
   hs.assign(nsys, BatchSys{});
-  int64_t ao = 0, co = 0, so = 0, go = 0, xo = 0, max_pb = 1;
+  int64_t ao = 0, co = 0, so = 0, go = 0, xo = 0;
+  int pb = 0, planes = 0;
   for (int i = 0; i < nsys; ++i) {
     const int64_t n = natoms[i];
     const int K = pme_grid[i];
@@ -185,7 +198,10 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
     y.mod_off = moduli_offset(K);
     const int64_t ncplx = (int64_t)K * K * (K / 2 + 1);
     y.pme_blocks = (int)std::min<int64_t>(kBatchPmeMaxBlocks, std::max<int64_t>(1, (std::max(n * kLanesPerAtom, ncplx) + kPmeBlock - 1) / kPmeBlock));
-    max_pb = std::max<int64_t>(max_pb, y.pme_blocks);
+    y.pb_off = pb;
+    y.plane_off = planes;
+    pb += y.pme_blocks;
+    planes += K;
     ao += n;
     co += y.ncl;
     so += y.nsup;
@@ -201,10 +217,35 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
   }
   TFF_ARG(go <= L.grid + 64 * L.systems, "batch holds %lld PME grid points; capacity %lld", (long long)go,
           (long long)L.grid);
-  const int64_t ncl = co, nsup = so, npad = co * kWarp, total_atoms = ao, total_grid = go;
+  BatchShape sh{};
+  sh.natoms = ao;
+  sh.nclusters = co;
+  sh.npad = co * kWarp;
+  sh.nsuper = so;
+  sh.total_grid = go;
+  sh.nsys = nsys;
+  sh.pb_units = pb;
+  sh.plane_units = planes;
+  sh.kmax = kmax;
+  // the pinned block is reused once the previous upload out of it is done
+  TFF_CUDA(cudaEventSynchronize(b->table_ev));
+  std::memcpy(b->table, &sh, sizeof(sh));
+  std::memcpy(b->table + kTableOffset, hs.data(), nsys * sizeof(BatchSys));
+  *kmax_out = kmax;
+  return TFF_OK;
+}
 
-  // --- device pointers
+// Device part of an evaluation on stream s (PME on the batch's second stream, joined back):
+// every launch shape depends on the batch's capacity and the DFT class alone, so the
+// sequence can be captured once and replayed for any composition of that class.
+template <class T>
+int batch_enqueue(tff_batch b, int kclass, const T *x, const T *boxes, const T *q, const T *sigma, const T *eps,
+                  const int *excl, double *energies, T *forces, cudaStream_t s) {
+  using S = typename Acc<T>::S;
+  const BatchLayout &L = b->L;
   char *w = b->ws;
+  const int sms = sm_count();
+  const int64_t slots_cap = L.clusters * kWarp;
   ClusterData<T> cd{};
   using V = typename V4<T>::type;
   cd.status = reinterpret_cast<unsigned *>(w + L.status);
@@ -222,84 +263,93 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
   cd.sbh = reinterpret_cast<V *>(w + L.sbh);
   cd.boxinfo = reinterpret_cast<double *>(w + L.boxinfo);
   cd.cap = L.cap;
-  cd.natoms = total_atoms;
-  cd.nclusters = ncl;
-  cd.npad = npad;
-  cd.nsuper = nsup;
+  // sizes come from the shape on the device; the capacities stand here
+  cd.natoms = L.atoms;
+  cd.nclusters = L.clusters;
+  cd.npad = slots_cap;
+  cd.nsuper = L.supers;
   cd.sys = reinterpret_cast<const BatchSys *>(w + L.sys);
   cd.cl_sys = reinterpret_cast<int *>(w + L.cl_sys);
   cd.sup_sys = reinterpret_cast<int *>(w + L.sup_sys);
+  cd.shape = reinterpret_cast<const BatchShape *>(w + L.shape);
+  const BatchShape *shape = cd.shape;
+  const BatchSys *dsys = cd.sys;
 
-  // --- upload the table (the pinned buffer is reused once the previous upload is done)
-  TFF_CUDA(cudaEventSynchronize(b->table_ev));
-  std::copy(hs.begin(), hs.end(), b->table);
-  TFF_CUDA(cudaMemcpyAsync(w + L.sys, b->table, nsys * sizeof(BatchSys), cudaMemcpyHostToDevice, s));
-  TFF_CUDA(cudaEventRecord(b->table_ev, s));
   TFF_CUDA(cudaMemsetAsync(w + L.status, 0, 64 * sizeof(unsigned), s));
-  TFF_CUDA(cudaMemsetAsync(w + L.e_tile, 0, 2 * nsys * 8, s));
-  TFF_CUDA(cudaMemsetAsync(w + L.acc, 0, npad * 4 * 8, s));
-  const int sms = sm_count();
+  TFF_CUDA(cudaMemsetAsync(w + L.e_tile, 0, 2 * L.systems * 8, s));
 
   // --- PME on the side stream
   TFF_CUDA(cudaEventRecord(b->fork_ev, s));
   cudaStream_t ps = b->pme_stream;
   TFF_CUDA(cudaStreamWaitEvent(ps, b->fork_ev, 0));
-  TFF_CUDA(cudaMemsetAsync(w + L.fix, 0, total_grid * 8, ps));
-  TFF_CUDA(cudaMemsetAsync(w + L.tickets, 0, 2 * nsys * sizeof(unsigned), ps));
-  const BatchSys *dsys = cd.sys;
+  TFF_CUDA(cudaMemsetAsync(w + L.tickets, 0, 2 * L.systems * sizeof(unsigned), ps));
   double *partials = reinterpret_cast<double *>(w + L.partials);
   unsigned *tickets = reinterpret_cast<unsigned *>(w + L.tickets);
   double *e_pme = reinterpret_cast<double *>(w + L.e_pme);
   S *fix = reinterpret_cast<S *>(w + L.fix);
   T *pme_grad = reinterpret_cast<T *>(w + L.pme_grad);
   T *pme_phi = reinterpret_cast<T *>(w + L.pme_phi);
-  const dim3 pgrid((unsigned)max_pb, (unsigned)nsys);
-  batch_spread_kernel<T><<<pgrid, kPmeBlock, 0, ps>>>(dsys, x, q, boxes, fix);
+  const int nb_pme = sms * 8;
+  batch_zero_grid_kernel<S><<<sms * 8, 256, 0, ps>>>(shape, fix);
+  TFF_LAUNCHED();
+  // work-unit counters of the persistent PME kernels: status words 16.. (zeroed above)
+  unsigned *counters = cd.status + 16;
+  batch_spread_kernel<T><<<nb_pme, kPmeBlock, 0, ps>>>(dsys, shape, x, q, boxes, fix, counters);
   TFF_LAUNCHED();
   T *real;
   if (sizeof(T) == 4) {
     real = reinterpret_cast<T *>(w + L.real);
-    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((total_grid + 255) / 256, sms * 8));
-    pme_fix_to_real_kernel<<<nb, 256, 0, ps>>>(reinterpret_cast<unsigned long long *>(fix),
-                                               reinterpret_cast<float *>(real), total_grid);
+    batch_fix_to_real_kernel<<<sms * 8, 256, 0, ps>>>(shape, reinterpret_cast<unsigned long long *>(fix),
+                                                     reinterpret_cast<float *>(real));
     TFF_LAUNCHED();
   } else {
     real = reinterpret_cast<T *>(fix);
   }
   auto *cplx = reinterpret_cast<typename CplxOf<T>::type *>(w + L.cplx);
-  int st = run_dft<T>(dsys, nsys, kmax, true, real, cplx, ps);
-  if (st != TFF_OK) return st;
-  batch_convolve_kernel<T><<<pgrid, kPmeBlock, 0, ps>>>(dsys, cplx, boxes, b->desc.ewald_alpha,
-                                                        reinterpret_cast<const T *>(w + L.moduli), partials, tickets,
-                                                        e_pme);
+  const size_t dsmem = batch_dft_smem<T>(kclass);
+  const int nb_dft = sms * 8;
+  batch_dft_kernel<T, kDftZR2C><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 1);
   TFF_LAUNCHED();
-  if ((st = run_dft<T>(dsys, nsys, kmax, false, real, cplx, ps)) != TFF_OK) return st;
+  batch_dft_kernel<T, kDftY><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 2);
+  TFF_LAUNCHED();
+  batch_dft_kernel<T, kDftX><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 3);
+  TFF_LAUNCHED();
+  batch_convolve_kernel<T><<<nb_pme, kPmeBlock, 0, ps>>>(dsys, shape, cplx, boxes, b->desc.ewald_alpha,
+                                                         reinterpret_cast<const T *>(w + L.moduli), partials, tickets,
+                                                         e_pme, counters + 4);
+  TFF_LAUNCHED();
+  batch_dft_kernel<T, kDftXInv><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 5);
+  TFF_LAUNCHED();
+  batch_dft_kernel<T, kDftYInv><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 6);
+  TFF_LAUNCHED();
+  batch_dft_kernel<T, kDftZC2R><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 7);
+  TFF_LAUNCHED();
 
   // --- real space on the caller stream
-  batch_sort_kernel<T><<<(int)std::min<int64_t>(nsys, 2 * sms), kBatchSortThreads, kBatchSortSmem, s>>>(x, q, boxes,
-                                                                                                     nsys, cd);
+  S *gx = reinterpret_cast<S *>(w + L.acc);
+  S *gq = gx + 3 * slots_cap;
+  batch_sort_kernel<T><<<(int)std::min<int64_t>(L.systems, 2 * sms), kBatchSortThreads, kBatchSortSmem, s>>>(
+      x, q, boxes, cd, reinterpret_cast<unsigned long long *>(gx), slots_cap);
   TFF_LAUNCHED();
   // the PME gather follows the sort's atom order
   TFF_CUDA(cudaEventRecord(b->sorted_ev, s));
   TFF_CUDA(cudaStreamWaitEvent(ps, b->sorted_ev, 0));
-  batch_gather_kernel<T><<<pgrid, kPmeBlock, 0, ps>>>(dsys, x, q, cd.sidx, boxes, real, b->desc.ewald_alpha, pme_phi,
-                                                      pme_grad, partials, tickets, e_pme);
+  batch_gather_kernel<T><<<nb_pme, kPmeBlock, 0, ps>>>(dsys, shape, x, q, cd.sidx, boxes, real, b->desc.ewald_alpha,
+                                                       pme_phi, pme_grad, partials, tickets, e_pme, counters + 8);
   TFF_LAUNCHED();
   TFF_CUDA(cudaEventRecord(b->join_ev, ps));
-  cluster_bounds_kernel<T><<<(int)std::max<int64_t>(1, std::min<int64_t>(nsup, 2 * sms)), kWarp * kSuper, 0, s>>>(cd);
+  cluster_bounds_kernel<T><<<(int)std::max<int64_t>(1, std::min<int64_t>(L.supers, 2 * sms)), kWarp * kSuper, 0, s>>>(cd);
   TFF_LAUNCHED();
-  const int nb_cl = (int)std::max<int64_t>(1, std::min<int64_t>((ncl + 3) / 4, sms * 16));
+  const int nb_cl = (int)std::max<int64_t>(1, std::min<int64_t>((L.clusters + 3) / 4, sms * 16));
   cluster_neighbors_kernel<T><<<nb_cl, 128, 0, s>>>(cd, b->desc.cutoff, kHalfLists<T>);
   TFF_LAUNCHED();
   auto *lj = reinterpret_cast<typename V2<T>::type *>(w + L.lj);
   int *exslot = reinterpret_cast<int *>(w + L.exslot);
   {
-    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((npad + 255) / 256, sms * 8));
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((slots_cap + 255) / 256, sms * 8));
     sorted_params_kernel<T><<<nb, 256, 0, s>>>(cd, sigma, eps, excl, lj, exslot);
     TFF_LAUNCHED();
   }
-  S *gx = reinterpret_cast<S *>(w + L.acc);
-  S *gq = gx + 3 * npad;
   S *e_tile = reinterpret_cast<S *>(w + L.e_tile);
   {
     TileArgs<T> A;
@@ -312,16 +362,77 @@ int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme
     A.alpha = b->desc.ewald_alpha;
     A.kc = b->desc.coul_constant;
     A.energies = e_tile;
-    const int64_t max_items = ncl * ((L.cap + kItemTiles - 1) / kItemTiles);
+    const int64_t max_items = L.clusters * ((L.cap + kItemTiles - 1) / kItemTiles);
     const int st_rs = launch_real_space<T>(false, max_items, sms, s, A);
     if (st_rs != TFF_OK) return st_rs;
   }
   TFF_CUDA(cudaStreamWaitEvent(s, b->join_ev, 0));
-  const int nbf = (int)std::max<int64_t>(1, std::min<int64_t>((total_atoms + 255) / 256, sms * 8));
+  const int nbf = (int)std::max<int64_t>(1, std::min<int64_t>((L.atoms + 255) / 256, sms * 8));
   finalize_kernel<T><<<nbf, 256, 0, s>>>(cd, gx, gq, pme_grad, pme_phi, forces, (double *)nullptr, (T *)nullptr,
-                                         e_tile, e_pme, b->desc.coul_constant, energies, (double *)nullptr, nsys);
+                                         e_tile, e_pme, b->desc.coul_constant, energies, (double *)nullptr,
+                                         (int)L.systems);
   TFF_LAUNCHED();
   return TFF_OK;
+}
+
+// Most graphs a batch keeps (one per DFT class and buffer set; the oldest goes first).
+constexpr size_t kBatchMaxGraphs = 8;
+
+// Captures the device part for `key` (nothing runs) and appends the graph to the batch's
+// list.
+template <class T>
+int batch_capture(tff_batch b, const BatchGraphKey &key, const T *x, const T *boxes, const T *q, const T *sigma,
+                  const T *eps, const int *excl, double *energies, T *forces) {
+  if (b->capture_stream == nullptr) TFF_CUDA(cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking));
+  TFF_CUDA(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
+  const int st = batch_enqueue<T>(b, key.dft_class, x, boxes, q, sigma, eps, excl, energies, forces,
+                                  b->capture_stream);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(b->capture_stream, &graph);
+  if (st != TFF_OK || ee != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    if (st != TFF_OK) return st;
+    return cuda_fail(ee, "batch graph capture", __FILE__, __LINE__);
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+  if (b->graphs.size() >= kBatchMaxGraphs) {
+    cudaGraphExecDestroy(b->graphs.front().second);
+    b->graphs.erase(b->graphs.begin());
+  }
+  b->graphs.emplace_back(key, exec);
+  return TFF_OK;
+}
+
+template <class T>
+int batch_eval_impl(tff_batch b, int nsys, const int64_t *natoms, const int *pme_grid, const T *x, const T *boxes,
+                    const T *q, const T *sigma, const T *eps, const int *excl, double *energies, T *forces,
+                    cudaStream_t s) {
+  int kmax = 6;
+  int st = batch_prepare<T>(b, nsys, natoms, pme_grid, &kmax);
+  if (st != TFF_OK) return st;
+  const int kclass = dft_class(kmax, sizeof(T) == 8 ? kBatchMaxK64 : kBatchMaxK);
+  // upload the shape and the table (exact size), then run the device part
+  TFF_CUDA(cudaMemcpyAsync(b->ws + b->L.shape, b->table, kTableOffset + nsys * sizeof(BatchSys),
+                           cudaMemcpyHostToDevice, s));
+  TFF_CUDA(cudaEventRecord(b->table_ev, s));
+  const BatchGraphKey key{{x, boxes, q, sigma, eps, excl, energies, forces, nullptr, nullptr}, kclass};
+  auto it = std::find_if(b->graphs.begin(), b->graphs.end(), [&](const auto &g) { return g.first == key; });
+  if (it == b->graphs.end() && b->have_last && b->last_key == key) {
+    // the same buffers and class twice in a row: capture the device part once
+    if ((st = batch_capture<T>(b, key, x, boxes, q, sigma, eps, excl, energies, forces)) != TFF_OK) return st;
+    it = b->graphs.end() - 1;
+  }
+  b->last_key = key;
+  b->have_last = true;
+  if (it != b->graphs.end()) {
+    ++b->graph_launches;
+    TFF_CUDA(cudaGraphLaunch(it->second, s));
+    return TFF_OK;
+  }
+  return batch_enqueue<T>(b, kclass, x, boxes, q, sigma, eps, excl, energies, forces, s);
 }
 
 template <class T>
@@ -339,6 +450,22 @@ int set_sort_smem() {
 }
 
 }  // namespace
+
+// Captures the graph of the batch's common DFT class (grid sides up to 52) for these
+// device buffers ahead of use, so that the first evaluations through them need no capture
+// (used for the server's lanes, whose staging buffers never change).
+int batch_warm_graph(tff_batch b, const void *coords, const void *boxes, const void *charges, const void *sigma,
+                     const void *epsilon, const int *excl, double *energies, void *forces) {
+  const int kcap = b->desc.dtype == TFF_F64 ? kBatchMaxK64 : kBatchMaxK;
+  const BatchGraphKey key{{coords, boxes, charges, sigma, epsilon, excl, energies, forces, nullptr, nullptr},
+                          dft_class(6, kcap)};
+  if (b->desc.dtype == TFF_F32)
+    return batch_capture<float>(b, key, (const float *)coords, (const float *)boxes, (const float *)charges,
+                                (const float *)sigma, (const float *)epsilon, excl, energies, (float *)forces);
+  return batch_capture<double>(b, key, (const double *)coords, (const double *)boxes, (const double *)charges,
+                               (const double *)sigma, (const double *)epsilon, excl, energies, (double *)forces);
+}
+
 }  // namespace tff
 
 extern "C" {
@@ -367,7 +494,7 @@ int tff_batch_create(const tff_batch_desc *desc, tff_batch *out) {
   cudaGetDevice(&b->device);
   cudaError_t e = cudaMalloc(&b->ws, b->L.bytes);
   if (e == cudaSuccess) e = cudaMemset(b->ws, 0, b->L.bytes);
-  if (e == cudaSuccess) e = cudaMallocHost((void **)&b->table, desc->max_systems * sizeof(BatchSys));
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&b->table, kTableOffset + desc->max_systems * sizeof(BatchSys));
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->table_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->pme_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
@@ -434,11 +561,13 @@ int tff_batch_status(tff_batch b, tff_stream_t stream, int *status) {
   return TFF_OK;
 }
 
+int64_t tff_batch_graph_launches(tff_batch b) { return b ? b->graph_launches : 0; }
+
 int tff_batch_kernel_launches(tff_batch b) {
   if (!b) return 0;
-  // sort, bounds, neighbours, params, tile, finalize; spread, [to_real], 3 DFT passes,
-  // convolve, 3 inverse passes, gather
-  return 6 + (b->desc.dtype == TFF_F32 ? 10 : 9);
+  // sort, bounds, neighbours, params, pair kernel, finalize; grid zeroing, spread,
+  // [to_real], 3 DFT passes, convolve, 3 inverse passes, gather
+  return 6 + (b->desc.dtype == TFF_F32 ? 11 : 10);
 }
 
 }  // extern "C"

@@ -114,7 +114,21 @@ struct BatchSys {
   int64_t grid_off, cplx_off;  // PME grids: K^3 real points, K*K*(K/2+1) complex points
   int nc, bits;                // cell grid side and Hilbert bits per axis
   int K, mod_off;              // PME grid side and offset of its B-spline moduli
-  int pme_blocks, pad;         // blocks of the per-system PME reductions
+  int pme_blocks;              // blocks of the per-system PME reductions
+  int pb_off;                  // the system's first PME work unit (sum of pme_blocks before it)
+  int plane_off;               // the system's first DFT plane unit (sum of K before it)
+  int pad;
+};
+
+// Totals of a batch, in device memory beside its system table: the batched kernels read
+// the batch's composition here, so their launch shapes depend on the batch's capacity
+// alone and one captured CUDA graph serves every composition.
+struct BatchShape {
+  int64_t natoms, nclusters, npad, nsuper, total_grid;
+  int nsys;
+  int pb_units;     // PME work units: sum of pme_blocks
+  int plane_units;  // DFT plane units: sum of K
+  int kmax;
 };
 
 // Stride of the per-system box facts (see box_info_kernel).
@@ -138,7 +152,12 @@ struct ClusterData {
   const BatchSys *sys;
   int *cl_sys;   // owning system of each cluster
   int *sup_sys;  // owning system of each super-cluster
+  const BatchShape *shape;  // batch mode: the sizes below come from here (device memory)
   __device__ __forceinline__ int system_of(int64_t cluster) const { return cl_sys ? cl_sys[cluster] : 0; }
+  __device__ __forceinline__ int64_t n_atoms() const { return shape ? shape->natoms : natoms; }
+  __device__ __forceinline__ int64_t n_clusters() const { return shape ? shape->nclusters : nclusters; }
+  __device__ __forceinline__ int64_t n_pad() const { return shape ? shape->npad : npad; }
+  __device__ __forceinline__ int64_t n_super() const { return shape ? shape->nsuper : nsuper; }
   __device__ __forceinline__ const double *info(int system) const { return boxinfo + kInfoStride * system; }
 };
 
@@ -175,6 +194,7 @@ inline ClusterData<T> cluster_data(const ClusterLayout &L, void *ws) {
   d.sys = nullptr;
   d.cl_sys = nullptr;
   d.sup_sys = nullptr;
+  d.shape = nullptr;
   return d;
 }
 
@@ -416,7 +436,9 @@ __global__ void sort_buckets_kernel(const T *x, const T *q, int64_t nkeys, Clust
 // system's own Hilbert-ordered cell grid in shared memory (counting sort, then an
 // insertion sort of each bucket by atom index, which makes the order deterministic and
 // equal to the single-system sort), writes the sorted SoA with padding to whole clusters
-// and the cluster / super-cluster owners. Limits: kBatchMaxAtoms atoms and
+// and the cluster / super-cluster owners, and zeroes the energy kernel's accumulators of
+// those slots (acc: dE/dx of slots_cap slots, then dE/dq). The system count comes from
+// d.shape. Limits: kBatchMaxAtoms atoms and
 // kBatchMaxKeys keys per system (16 cells per side).
 constexpr int kBatchSortThreads = 1024;
 constexpr int kBatchMaxAtoms = 16384;
@@ -424,8 +446,9 @@ constexpr int kBatchMaxKeys = 4096;
 constexpr size_t kBatchSortSmem = (2 * kBatchMaxKeys + 1) * sizeof(unsigned) + 2 * kBatchMaxAtoms * sizeof(unsigned short);
 
 template <class T>
-__global__ void __launch_bounds__(kBatchSortThreads) batch_sort_kernel(const T *x, const T *q, const T *boxes, int nsys,
-                                                                       ClusterData<T> d) {
+__global__ void __launch_bounds__(kBatchSortThreads) batch_sort_kernel(const T *x, const T *q, const T *boxes,
+                                                                       ClusterData<T> d, unsigned long long *acc,
+                                                                       int64_t slots_cap) {
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned *hist = reinterpret_cast<unsigned *>(smem);          // kBatchMaxKeys + 1
   unsigned *fill = hist + kBatchMaxKeys + 1;                     // kBatchMaxKeys
@@ -434,6 +457,7 @@ __global__ void __launch_bounds__(kBatchSortThreads) batch_sort_kernel(const T *
   __shared__ double s_info[kInfoStride];
   __shared__ unsigned s_warp[32];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int nsys = d.shape->nsys;
   for (int sy = blockIdx.x; sy < nsys; sy += gridDim.x) {
     const BatchSys b = d.sys[sy];
     const int n = (int)b.natoms;
@@ -519,6 +543,11 @@ __global__ void __launch_bounds__(kBatchSortThreads) batch_sort_kernel(const T *
     const int npad = (int)(b.ncl * kWarp);
     for (int p = tid; p < npad; p += blockDim.x) {
       const int64_t slot = base + p;
+      // the energy kernel's accumulators of the slot: dE/dx (3 per slot), then dE/dq
+      acc[3 * slot] = 0ull;
+      acc[3 * slot + 1] = 0ull;
+      acc[3 * slot + 2] = 0ull;
+      acc[3 * slots_cap + slot] = 0ull;
       if (p < n) {
         const int t = order[p];
         const int64_t a = b.atom_off + t;
@@ -562,9 +591,10 @@ __global__ void __launch_bounds__(kWarp * kSuper) cluster_bounds_kernel(ClusterD
   pdl_enter();
   __shared__ double s_box[kSuper][6];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int64_t S = blockIdx.x; S < d.nsuper; S += gridDim.x) {
+  const int64_t nsuper = d.n_super();
+  for (int64_t S = blockIdx.x; S < nsuper; S += gridDim.x) {
     // members [first, last) of super-cluster S, all in one system
-    int64_t first = S * kSuper, last = min(first + kSuper, d.nclusters);
+    int64_t first = S * kSuper, last = min(first + kSuper, d.n_clusters());
     int sy = 0;
     if (d.sys) {
       sy = d.sup_sys[S];
@@ -705,12 +735,13 @@ __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) 
   pdl_enter();
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t I = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); I < d.nclusters; I += nw) {
+  const int64_t ncl = d.n_clusters();
+  for (int64_t I = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); I < ncl; I += nw) {
     const auto ci = d.bc[I];
     const auto hi = d.bh[I];
     int count = 0;
     // candidates: clusters [j0, jend) and super-clusters [s0, send) of I's system
-    int64_t j0 = 0, j1 = d.nclusters, s0 = 0;
+    int64_t j0 = 0, j1 = ncl, s0 = 0;
     int sy = 0;
     if (d.sys) {
       sy = d.cl_sys[I];
@@ -787,7 +818,7 @@ __global__ void cluster_neighbors_kernel(ClusterData<T> d, double rc, int half) 
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  const int64_t n = d.nclusters;
+  const int64_t n = ncl;
   const int64_t per = (n + blockDim.x - 1) / blockDim.x;
   const int64_t beg = min((int64_t)threadIdx.x * per, n), end = min(beg + per, n);
   int sum = 0;

@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
   const T two_a_rpi = (T)(2.0 * A.alpha / 1.7724538509055160273);
   const T far = sizeof(T) == 4 ? T(1e18) : T(1e150);  // padding slots: outside every cutoff
 
-  const int nitems = cl.itemoff[cl.nclusters];
+  const int nitems = cl.itemoff[cl.n_clusters()];
   const int nwarps = gridDim.x * NW;
   for (int it = blockIdx.x * NW + w; it < nitems; it += nwarps) {
     const int I = cl.items[it];  // owning cluster: itemoff[I] <= it < itemoff[I + 1]

@@ -466,8 +466,9 @@ __global__ void __launch_bounds__(kPmeBlock) pme_gather_hvp_kernel(PlainAtoms<T>
 }
 
 // ---- batched 3-D real DFT of many grids of different sizes (the serving path)
-// One launch per axis pass over every system of a batch: blockIdx.y = system, blockIdx.x =
-// plane (0..K-1). A block stages one plane in shared memory as `lines` x `points` with an
+// One launch per axis pass over every system of a batch. The work units are the planes of
+// every grid (system s owns units plane_off .. plane_off + K - 1); blocks loop over them.
+// A block stages one plane in shared memory as `lines` x `points` with an
 // odd row stride (so lanes reading one point of consecutive lines hit distinct banks),
 // evaluates each output as a direct sum over the line with a twiddle table
 // w[m] = exp(-+2 pi i m / K) (consecutive lanes share the twiddle: a broadcast), stages
@@ -486,14 +487,40 @@ inline size_t batch_dft_smem(int K) {
   return (size_t)(K + 2 * (size_t)K * dft_stride(K)) * 2 * sizeof(T);
 }
 
+// Next work unit of a persistent batched kernel, drawn from a per-launch counter (zeroed
+// before the launch) so that blocks that finish early take more: returns the unit, equal
+// to `units` or more when none is left. Called by every thread of the block; the first
+// barrier also keeps the previous unit's shared memory until every thread is done with it.
+__device__ __forceinline__ int next_unit(unsigned *counter) {
+  __shared__ int s_unit;
+  __syncthreads();
+  if (threadIdx.x == 0) s_unit = (int)atomicAdd(counter, 1u);
+  __syncthreads();
+  return s_unit;
+}
+
+// The batch system owning work unit u: the largest s < nsys whose first unit (plane_off for
+// DFT planes, pb_off for PME blocks) is at most u. Every system owns at least one unit.
+template <bool PLANES>
+__device__ __forceinline__ int unit_system(const BatchSys *sys, int nsys, int u) {
+  int lo = 0, hi = nsys - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const int off = PLANES ? sys[mid].plane_off : sys[mid].pb_off;
+    if (off <= u)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// One plane p of one grid (see batch_dft_kernel).
 template <class T, int PASS>
-__global__ void __launch_bounds__(kDftThreads) batch_dft_kernel(const BatchSys *sys, T *real,
-                                                                typename CplxOf<T>::type *cplx) {
+__device__ __forceinline__ void batch_dft_plane(const BatchSys &b, const int p, T *real, typename CplxOf<T>::type *cplx) {
   using C = typename CplxOf<T>::type;
-  const BatchSys &b = sys[blockIdx.y];
   const int K = b.K;
-  if ((int)blockIdx.x >= K) return;
-  const int Kz = K / 2 + 1, st = dft_stride(K), p = blockIdx.x;
+  const int Kz = K / 2 + 1, st = dft_stride(K);
   constexpr bool kInverse = PASS >= kDftXInv;
   extern __shared__ __align__(16) unsigned char dft_smem[];
   C *tw = reinterpret_cast<C *>(dft_smem);
@@ -584,63 +611,109 @@ __global__ void __launch_bounds__(kDftThreads) batch_dft_kernel(const BatchSys *
   }
 }
 
-// ---- batched PME: blockIdx.y is the system, blocks [0, BatchSys::pme_blocks) of it work
-// (a count that depends on the system alone, so that its reductions sum in the same order
-// whatever else is in the batch).
+template <class T, int PASS>
+__global__ void __launch_bounds__(kDftThreads) batch_dft_kernel(const BatchSys *sys, const BatchShape *shape, T *real,
+                                                                typename CplxOf<T>::type *cplx, unsigned *counter) {
+  const int nsys = shape->nsys, units = shape->plane_units;
+  for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
+    const BatchSys &b = sys[unit_system<true>(sys, nsys, u)];
+    batch_dft_plane<T, PASS>(b, u - b.plane_off, real, cplx);
+  }
+}
+
+// ---- batched PME: the work units are the PME blocks of every system (system s owns units
+// pb_off .. pb_off + pme_blocks - 1; pme_blocks depends on the system alone, so that its
+// reductions sum in the same order whatever else is in the batch); blocks loop over them.
+// The spread and the convolution keep 4 resident blocks per SM (at most 64 registers): the
+// loop's extra state cost them a block per SM and 29 % / 67 % of their time at 256 systems.
 constexpr int kBatchPmeMaxBlocks = 256;
 
+// Zeroes the batch's accumulation grid (total_grid points of the shape).
+template <class S>
+__global__ void batch_zero_grid_kernel(const BatchShape *shape, S *grid) {
+  const int64_t n = shape->total_grid;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    grid[k] = S(0);
+}
+
+static __global__ void batch_fix_to_real_kernel(const BatchShape *shape, const unsigned long long *gi, float *gf) {
+  const int64_t n = shape->total_grid;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    gf[k] = (float)from_fix(gi[k]);
+}
+
+// One PME block of one system (a separate call: the unit loop's state then does not share
+// the inner loops' register allocation).
 template <class T>
-__global__ void __launch_bounds__(kPmeBlock) batch_spread_kernel(const BatchSys *sys, const T *x, const T *q,
-                                                                 const T *boxes, typename Acc<T>::S *grid) {
-  const BatchSys &b = sys[blockIdx.y];
-  if (blockIdx.x >= (unsigned)b.pme_blocks) return;
-  __shared__ PmeShared sh;
-  if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)blockIdx.y, b.K, sh);
+__device__ __noinline__ void batch_spread_unit(const BatchSys *sys, const T *x, const T *q, const T *boxes,
+                                               typename Acc<T>::S *grid, int sy, int bx, PmeShared &sh) {
+  const BatchSys &b = sys[sy];
+  if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
   __syncthreads();
   PlainAtoms<T> atoms{x + 3 * b.atom_off, q + b.atom_off, b.natoms};
-  spread_atoms<T>(atoms, b.natoms, sh, b.K, grid + b.grid_off, blockIdx.x, b.pme_blocks);
+  spread_atoms<T>(atoms, b.natoms, sh, b.K, grid + b.grid_off, bx, b.pme_blocks);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kPmeBlock, 4) batch_spread_kernel(const BatchSys *sys, const BatchShape *shape,
+                                                                 const T *x, const T *q, const T *boxes,
+                                                                 typename Acc<T>::S *grid, unsigned *counter) {
+  __shared__ PmeShared sh;
+  const int nsys = shape->nsys, units = shape->pb_units;
+  for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
+    const int sy = unit_system<false>(sys, nsys, u);
+    batch_spread_unit<T>(sys, x, q, boxes, grid, sy, u - sys[sy].pb_off, sh);
+  }
 }
 
 // partials: kBatchPmeMaxBlocks per system; tickets and energies: 2 per system
 // ([2s] reciprocal, [2s+1] self).
 template <class T>
-__global__ void __launch_bounds__(kPmeBlock) batch_convolve_kernel(const BatchSys *sys, typename CplxOf<T>::type *S,
-                                                                   const T *boxes, double alpha, const T *moduli,
-                                                                   double *partials, unsigned *tickets,
-                                                                   double *energies) {
-  const int sy = blockIdx.y;
-  const BatchSys &b = sys[sy];
-  if (blockIdx.x >= (unsigned)b.pme_blocks) return;
+__global__ void __launch_bounds__(kPmeBlock, 4) batch_convolve_kernel(const BatchSys *sys, const BatchShape *shape,
+                                                                   typename CplxOf<T>::type *S, const T *boxes,
+                                                                   double alpha, const T *moduli, double *partials,
+                                                                   unsigned *tickets, double *energies,
+                                                                   unsigned *counter) {
   __shared__ PmeShared sh;
-  if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
-  __syncthreads();
-  const T *xm = moduli + b.mod_off, *ym = xm + b.K, *zm = ym + b.K;
-  const double e = convolve_points<T>(S + b.cplx_off, sh, b.K, alpha, xm, ym, zm, blockIdx.x, b.pme_blocks);
-  grid_sum_n<kPmeBlock>(0.5 * e, partials + (int64_t)kBatchPmeMaxBlocks * sy, tickets + 2 * sy, energies + 2 * sy,
-                        false, blockIdx.x, b.pme_blocks);
+  const int nsys = shape->nsys, units = shape->pb_units;
+  for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
+    const int sy = unit_system<false>(sys, nsys, u);
+    const BatchSys &b = sys[sy];
+    const int bx = u - b.pb_off;
+    if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
+    __syncthreads();
+    const T *xm = moduli + b.mod_off, *ym = xm + b.K, *zm = ym + b.K;
+    const double e = convolve_points<T>(S + b.cplx_off, sh, b.K, alpha, xm, ym, zm, bx, b.pme_blocks);
+    grid_sum_n<kPmeBlock>(0.5 * e, partials + (int64_t)kBatchPmeMaxBlocks * sy, tickets + 2 * sy, energies + 2 * sy,
+                          false, bx, b.pme_blocks);
+  }
 }
 
 template <class T>
 // The atoms of a system are visited in the cluster order of the batch's sort (sidx: sorted
 // slot -> batch atom index, -1 for padding), so that neighbouring threads read neighbouring
 // grid points; each atom's numbers are those of the caller-order visit.
-__global__ void __launch_bounds__(kPmeBlock) batch_gather_kernel(const BatchSys *sys, const T *x, const T *q,
-                                                                 const int *sidx, const T *boxes, const T *Phi,
-                                                                 double alpha, T *phi, T *grad, double *partials,
-                                                                 unsigned *tickets, double *energies) {
-  const int sy = blockIdx.y;
-  const BatchSys &b = sys[sy];
-  if (blockIdx.x >= (unsigned)b.pme_blocks) return;
+__global__ void __launch_bounds__(kPmeBlock) batch_gather_kernel(const BatchSys *sys, const BatchShape *shape,
+                                                                 const T *x, const T *q, const int *sidx,
+                                                                 const T *boxes, const T *Phi, double alpha, T *phi,
+                                                                 T *grad, double *partials, unsigned *tickets,
+                                                                 double *energies, unsigned *counter) {
   __shared__ PmeShared sh;
-  if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
-  __syncthreads();
-  const int *slots = sidx + b.cl_off * kWarp;
-  const int64_t nslots = b.ncl * kWarp;
-  IndexedAtoms<T> atoms{x, q, slots, nslots};
-  IndexedGatherOut<T> out{phi, grad, slots};
-  const double e = gather_atoms<T>(atoms, nslots, sh, b.K, Phi + b.grid_off, alpha, out, blockIdx.x, b.pme_blocks);
-  grid_sum_n<kPmeBlock>(e, partials + (int64_t)kBatchPmeMaxBlocks * sy, tickets + 2 * sy + 1, energies + 2 * sy + 1,
-                        false, blockIdx.x, b.pme_blocks);
+  const int nsys = shape->nsys, units = shape->pb_units;
+  for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
+    const int sy = unit_system<false>(sys, nsys, u);
+    const BatchSys &b = sys[sy];
+    const int bx = u - b.pb_off;
+    if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
+    __syncthreads();
+    const int *slots = sidx + b.cl_off * kWarp;
+    const int64_t nslots = b.ncl * kWarp;
+    IndexedAtoms<T> atoms{x, q, slots, nslots};
+    IndexedGatherOut<T> out{phi, grad, slots};
+    const double e = gather_atoms<T>(atoms, nslots, sh, b.K, Phi + b.grid_off, alpha, out, bx, b.pme_blocks);
+    grid_sum_n<kPmeBlock>(e, partials + (int64_t)kBatchPmeMaxBlocks * sy, tickets + 2 * sy + 1,
+                          energies + 2 * sy + 1, false, bx, b.pme_blocks);
+  }
 }
 
 // Scratch layout of one PME evaluation.

@@ -402,6 +402,12 @@ int tff_server_create(const tff_server_desc *desc, tff_server *out) {
     if (st == TFF_OK && e == cudaSuccess) e = cudaMallocHost((void **)&l.h_out, l.out_bytes);
     if (st == TFF_OK && e == cudaSuccess) e = cudaMalloc((void **)&l.d_in, l.in_bytes);
     if (st == TFF_OK && e == cudaSuccess) e = cudaMalloc((void **)&l.d_out, l.out_bytes);
+    // the lane's staging buffers never change: its graph of the common DFT class is
+    // captured now rather than on the way of the first requests
+    if (st == TFF_OK && e == cudaSuccess)
+      st = batch_warm_graph(l.batch, l.d_in + l.o_x, l.d_in + l.o_box, l.d_in + l.o_q, l.d_in + l.o_s,
+                            l.d_in + l.o_e, reinterpret_cast<const int *>(l.d_in + l.o_excl),
+                            reinterpret_cast<double *>(l.d_out), l.d_out + l.o_f);
     if (st != TFF_OK || e != cudaSuccess) {
       if (st == TFF_OK) st = cuda_fail(e, "server lane set-up", __FILE__, __LINE__);
       free_server(s);

@@ -334,4 +334,8 @@ __device__ __forceinline__ void bspline6_d2(T w, T val[6], T der[6], T dd[6]) {
   }
 }
 
+// Server lanes: capture a batch's graph for its common DFT class ahead of use (batch.cu).
+int batch_warm_graph(tff_batch b, const void *coords, const void *boxes, const void *charges, const void *sigma,
+                     const void *epsilon, const int *excl, double *energies, void *forces);
+
 }  // namespace tff

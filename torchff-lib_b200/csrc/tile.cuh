@@ -83,7 +83,8 @@ __global__ void sorted_params_kernel(ClusterData<T> cl, const T *sigma, const T 
                                      typename V4<T>::type *dir_sorted = nullptr, typename Acc<T>::S *gx = nullptr,
                                      typename Acc<T>::S *gq = nullptr) {
   pdl_enter();
-  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < cl.npad; s += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t npad = cl.n_pad();
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < npad; s += (int64_t)gridDim.x * blockDim.x) {
     if (gx) {
       gx[3 * s] = 0;
       gx[3 * s + 1] = 0;
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(TileCfg<T, MODE>::NW * 32, MODE == 0 ? MIN_BLO
   const T kc = (T)A.kc;
   const T two_a_rpi = (T)(2.0 * A.alpha / 1.7724538509055160273);
 
-  const int nitems = cl.itemoff[cl.nclusters];
+  const int nitems = cl.itemoff[cl.n_clusters()];
   const int nwarps = gridDim.x * NW;
   for (int it = blockIdx.x * NW + w; it < nitems; it += nwarps) {
     const int I = cl.items[it];  // owning cluster: itemoff[I] <= it < itemoff[I + 1]
@@ -603,7 +604,9 @@ __global__ void finalize_kernel(ClusterData<T> cl, const typename Acc<T>::S *gx,
   // the build's overflow word (bit 0: a cluster's neighbour list was cut at its capacity),
   // copied out for a host caller that reads it together with the energy
   if (status_out && blockIdx.x == 0 && threadIdx.x == 0) *status_out = cl.status[0];
-  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < cl.natoms;
+  const int64_t natoms = cl.n_atoms();
+  if (cl.shape) nsys = cl.shape->nsys;
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < natoms;
        a += (int64_t)gridDim.x * blockDim.x) {
     const int64_t s = cl.inv[a];
     double x = Acc<T>::get(&gx[3 * s]), y = Acc<T>::get(&gx[3 * s + 1]), z = Acc<T>::get(&gx[3 * s + 2]);
@@ -635,8 +638,8 @@ __global__ void finalize_kernel(ClusterData<T> cl, const typename Acc<T>::S *gx,
     const double e_tile[2] = {Acc<T>::get(&e_tile_acc[2 * sy]), Acc<T>::get(&e_tile_acc[2 * sy + 1])};
     const double rec = e_pme ? kc * e_pme[2 * sy] : 0.0;
     const double self = e_pme ? kc * e_pme[2 * sy + 1] : 0.0;
-    const double eb = bonded ? Acc<T>::get(&bonded[3 * cl.natoms]) : 0.0;
-    const double ea = bonded ? Acc<T>::get(&bonded[3 * cl.natoms + 1]) : 0.0;
+    const double eb = bonded ? Acc<T>::get(&bonded[3 * natoms]) : 0.0;
+    const double ea = bonded ? Acc<T>::get(&bonded[3 * natoms + 1]) : 0.0;
     const double tot = e_tile[0] + e_tile[1] + rec + self + eb + ea;
     if (energy) energy[sy] = tot;
     if (terms) {

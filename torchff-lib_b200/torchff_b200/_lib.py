@@ -114,6 +114,7 @@ _SIGS = {
     "tff_batch_eval": (i32, [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "tff_batch_status": (i32, [vp, vp, C.POINTER(C.c_int)]),
     "tff_batch_kernel_launches": (i32, [vp]),
+    "tff_batch_graph_launches": (C.c_int64, [vp]),
     "tff_server_create": (i32, [C.POINTER(ServerDesc), C.POINTER(vp)]),
     "tff_server_destroy": (i32, [vp]),
     "tff_server_submit": (i32, [vp, C.POINTER(RequestDesc), C.POINTER(i64)]),

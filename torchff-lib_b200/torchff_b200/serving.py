@@ -101,6 +101,11 @@ class BatchEvaluator:
     def kernel_launches(self) -> int:
         return int(lib.tff_batch_kernel_launches(self._h))
 
+    def graph_launches(self) -> int:
+        """Evaluations so far that replayed a captured CUDA graph (evaluate_packed on the
+        same device buffers and DFT size class as the call before captures one)."""
+        return int(lib.tff_batch_graph_launches(self._h))
+
     def pack(self, systems: list[SystemSpec]) -> dict:
         """Device tensors of a batch (systems one after another), reusable across calls."""
         dev, dt = self.device, self.dtype
