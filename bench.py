@@ -732,7 +732,7 @@ def run_ours(args):
                 result["speedup_vs_reference_fp64_cuda"] = {
                     "device": round(value / rg["value"], 2), "e2e": round(e2e_value / rg["value"], 2),
                     "formula": "this line's value (and e2e value) / reference_gpu.value (the reference's FP64 CUDA "
-                               "ops on the same box and GPU, CUDA graph, L2 flushed)"}
+                               f"ops on the same box and GPU, {rg['fp64']['mode']}, L2 flushed)"}
         clocks.stop()
         result["clocks"] = clocks.summary()
         result["clocks_whole_run"] = dict(clocks.summary((run_t0, datetime.datetime.now())), note=(
@@ -932,13 +932,15 @@ def run_reference_gpu(args):
                    "path": "reference CUDA ops (oracle/_ref): build_neighbor_list_cell_list + "
                            "compute_lennard_jones_energy (type tables) + compute_multipolar_energy_from_atom_pairs "
                            "(rank 0, pairs_excl) + 138.935456 x pme_long_range, energy + backward",
-                   "timing": f"{r['fp64_timing_mode']}, {r['l2']}"},
+                   "timing": f"{r['fp64_timing_mode']}, {r['l2']}, median of the per-step CUDA-event times"},
         "fp64": {"evals_per_s": round(r["fp64_evals_per_s"], 2), "ms_per_eval": round(r["fp64_ms_per_eval"], 5),
                  "mode": r["fp64_timing_mode"], "capture_error": r.get("fp64_capture_error"),
+                 "ms_spread": {k: round(v, 5) for k, v in r["fp64_ms_spread"].items()},
                  "energy_rel_err_vs_oracle": r.get("fp64_energy_rel_err_vs_oracle"),
                  "force_rel_rms_vs_oracle": r.get("fp64_force_rel_rms_vs_oracle")},
         "fp32": {"evals_per_s": round(r["fp32_evals_per_s"], 2), "ms_per_eval": round(r["fp32_ms_per_eval"], 5),
                  "mode": r["fp32_timing_mode"], "capture_error": r.get("fp32_capture_error"),
+                 "ms_spread": {k: round(v, 5) for k, v in r["fp32_ms_spread"].items()},
                  "energy_rel_err_vs_oracle": r.get("fp32_energy_rel_err_vs_oracle"),
                  "force_rel_rms_vs_oracle": r.get("fp32_force_rel_rms_vs_oracle")},
         "clocks": clocks.summary(),

@@ -102,15 +102,18 @@ def energy(wb, d):
     return e_lj + e_c + e_p
 
 
-def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tuple[float, str, str]:
-    """ms per forward + backward: CUDA-graph replay as in torchff/test_utils.py:52-146, or,
+def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tuple[list, str, str]:
+    """ms of each of `steps` forwards + backwards: CUDA-graph replay as in torchff/test_utils.py:52-146, or,
     when the composition cannot be captured, eager calls. With flush_l2 a 256 MiB device
     write (larger than the 126 MB L2) runs before every timed replay, outside its events.
 
     Capture is tried in torch's "global", "thread_local" and "relaxed" error modes in turn.
-    A captured graph is used only if one replay reproduces the eager energy and forces to
-    1e-12, i.e. the graph does the whole evaluation. Returns (ms, mode, the capture errors
-    of the modes that failed)."""
+    A captured graph is used only if one replay reproduces the eager energy and forces, i.e.
+    the graph does the whole evaluation. The reference's ops accumulate with atomics (and
+    the LJ force accumulation races, so eager forces differ from call to call), so
+    "reproduces" means: within 1e-12 relative, or within 4x the largest difference seen
+    between three eager calls. Returns (per-step ms, mode, the capture errors of the
+    modes that failed)."""
     import torch
 
     x = d["coords"]
@@ -122,11 +125,16 @@ def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tup
             energy(wb, d).backward()
     torch.cuda.current_stream().wait_stream(s)
     torch.cuda.synchronize()
-    x.grad = None
-    e_ref = energy(wb, d)
-    e_ref.backward()
-    e_ref = float(e_ref.item())
-    g_ref = x.grad.detach().clone()
+    eager = []
+    for _ in range(3):
+        x.grad = None
+        e = energy(wb, d)
+        e.backward()
+        eager.append((float(e.item()), x.grad.detach().clone()))
+    e_ref, g_ref = eager[0]
+    e_tol = 1e-12 * abs(e_ref) + 4 * max(abs(ei - ej) for ei, _ in eager for ej, _ in eager)
+    g_tol = 1e-12 * float(g_ref.abs().max()) + 4 * max(float((gi - gj).abs().max()) for _, gi in eager
+                                                         for _, gj in eager)
     flush = torch.empty(256 * 1024 * 1024 if flush_l2 else 1, dtype=torch.uint8, device="cuda")
     a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     errors = []
@@ -140,8 +148,8 @@ def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tup
                 e.backward()
             g.replay()
             torch.cuda.synchronize()
-            same = (abs(float(e.item()) - e_ref) <= 1e-12 * abs(e_ref)
-                    and float((x.grad - g_ref).abs().max()) <= 1e-12 * float(g_ref.abs().max()))
+            same = (abs(float(e.item()) - e_ref) <= e_tol
+                    and float((x.grad - g_ref).abs().max()) <= g_tol)
             if not same:
                 errors.append(f"{cmode}: captured, but a replay does not reproduce the eager result")
                 continue
@@ -158,15 +166,15 @@ def time_graph(wb, d, steps: int, warmup: int = 5, flush_l2: bool = True) -> tup
         def run():
             x.grad = None
             energy(wb, d).backward()
-    total = 0.0
+    times = []
     for i in range(steps):
         flush.fill_(i & 0xff)
         a.record()
         run()
         z.record()
         z.synchronize()
-        total += a.elapsed_time(z)
-    return total / steps, mode, "; ".join(errors)
+        times.append(a.elapsed_time(z))
+    return times, mode, "; ".join(errors)
 
 
 def measure(workload: str = "water3000", steps: int = 200, warmup: int = 5, check: bool = True,
@@ -188,8 +196,13 @@ def measure(workload: str = "water3000", steps: int = 200, warmup: int = 5, chec
         e.backward()
         out[f"{name}_energy"] = float(e.item())
         forces[name] = (-d["coords"].grad).double().cpu().numpy()
-        ms, mode, error = time_graph(wb, d, steps, warmup, flush_l2)
+        times, mode, error = time_graph(wb, d, steps, warmup, flush_l2)
+        # eager calls are bounded by the host (the ops synchronise), whose share of the box
+        # varies from run to run: the median step is the figure, the spread is reported beside it
+        ms = float(np.median(times))
         out[f"{name}_ms_per_eval"], out[f"{name}_timing_mode"] = ms, mode
+        out[f"{name}_ms_spread"] = {"mean": float(np.mean(times)), "p10": float(np.percentile(times, 10)),
+                                    "p90": float(np.percentile(times, 90)), "min": float(np.min(times))}
         if error:
             out[f"{name}_capture_error"] = error
         out[f"{name}_evals_per_s"] = 1e3 / ms

@@ -73,3 +73,29 @@ def test_mixed_precision_is_deterministic_and_accurate():
     assert torch.equal(res[0][0], res[1][0]) and torch.equal(res[0][1], res[1][1])
     assert rel(res[0][0].item(), e0) < 2e-6
     assert rel_rms(res[0][1], gx0) < 1e-5
+
+
+def test_mixed_spread_grid_does_not_depend_on_atom_order():
+    """The FP32 spread sums each group of three consecutive atoms (a water here) over the
+    union window of their stencils, and spreads atoms whose group is too spread out one by
+    one; either way every contribution is rounded to fixed point alone and the integers are
+    summed. A random permutation of the atoms breaks the groups apart (other code paths, other
+    atomics), yet the grid, and so the energy and the forces, must be bit-identical."""
+    from torchff_b200.pme import PME
+    from torchff_b200.water import water_box_3000
+
+    wb = water_box_3000()
+    perm = np.random.default_rng(5).permutation(wb.natoms)
+    inv = np.argsort(perm)
+    pme = PME(wb.alpha, wb.grid, 0, use_customized_ops=True).cuda()
+    out = []
+    for order in (np.arange(wb.natoms), perm):
+        x = t(wb.coords[order], torch.float32, grad=True)
+        q = t(wb.charges[order], torch.float32, grad=True)
+        e = pme(x, t(wb.box, torch.float32), q)
+        e.backward()
+        out.append((e.detach().cpu(), x.grad.cpu(), q.grad.cpu()))
+    back = torch.as_tensor(inv)
+    assert torch.equal(out[0][0], out[1][0])
+    assert torch.equal(out[0][1], out[1][1][back])
+    assert torch.equal(out[0][2], out[1][2][back])

@@ -16,6 +16,8 @@
 
 #include <cufft.h>
 
+#include <type_traits>
+
 #include "cluster.cuh"
 
 namespace tff {
@@ -147,6 +149,163 @@ __device__ __forceinline__ void spread_atoms(const Atoms &atoms, int64_t nthread
       }
     }
   }
+}
+
+// Spread in groups of kSpreadGroup consecutive atoms (FP32 inputs, fixed-point grid). The
+// atoms of a molecule are usually consecutive (a water's O, H, H), so their 6x6x6 stencils
+// overlap: a warp sums a group's contributions over the union window of its stencils (at
+// most kSpreadWin points per axis) and adds each window point to the grid with one atomic,
+// where the per-atom spread adds every contribution (3 x 216 for a water, against 7^3 = 343
+// window points for a typical one). Every contribution is rounded to fixed point by itself
+// and the integers are summed, exactly as the per-atom spread's atomics sum them, so the
+// grid is bit-identical to it. A group whose atoms lie too far apart on the grid (or whose
+// stencils are taken on a grid of fewer than kSpreadWin points) is spread atom by atom.
+constexpr int kSpreadGroup = 3;
+constexpr int kGroupsPerPass = 10;  // most groups staged per warp and pass: 30 atoms, one per lane
+constexpr int kSpreadWin = 8;
+
+struct GroupStencil {
+  int org[3];    // first stencil point per axis, unwrapped: ceil(u) - 3
+  float w[3][6]; // B-spline weights
+  float q;
+  int valid;
+};
+
+// Grouped spread of atoms [0, n) by the blocks bid of nblk (warp-strided over groups); S is
+// the warp's stencil staging (kSpreadGroup * kGroupsPerPass entries in shared memory). Each
+// warp stages as many groups per pass as it takes for the groups to fill the warps.
+template <class Atoms>
+__device__ __forceinline__ void spread_groups(const Atoms &atoms, int64_t n, const PmeShared &sh, int K,
+                                              unsigned long long *grid, int64_t bid, int64_t nblk, GroupStencil *S) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wg = (bid * blockDim.x + threadIdx.x) / kWarp;
+  const int64_t nw = nblk * blockDim.x / kWarp;
+  const int64_t groups = (n + kSpreadGroup - 1) / kSpreadGroup;
+  const int gpp = (int)min((int64_t)kGroupsPerPass, max((int64_t)1, (groups + nw - 1) / nw));
+  const int kAtoms = kSpreadGroup * gpp;
+  for (int64_t base = wg * kAtoms; base < n; base += nw * kAtoms) {
+    __syncwarp();  // every lane is done with the previous pass's stencils
+    if (lane < kAtoms) {
+      GroupStencil &g = S[lane];
+      double rx, ry, rz;
+      float qa;
+      const int64_t a = base + lane;
+      g.valid = a < n && atoms.get(a, rx, ry, rz, qa);
+      if (g.valid) {
+        const double r[3] = {rx, ry, rz};
+        float der[6];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double u = sh.recip[3 * d] * r[0] + sh.recip[3 * d + 1] * r[1] + sh.recip[3 * d + 2] * r[2];
+          const double m0 = ceil(u);
+          bspline6<float>((float)(m0 - u), g.w[d], der);
+          g.org[d] = (int)m0 - 3;
+        }
+        g.q = qa;
+      }
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int gi = 0; gi < gpp; ++gi) {
+      const GroupStencil *G = S + kSpreadGroup * gi;
+      // offsets of the atoms' stencils from the first valid atom's, taken modulo K into
+      // (-K/2, K/2], and the window's extent per axis
+      int first = -1;
+#pragma unroll
+      for (int k = kSpreadGroup - 1; k >= 0; --k)
+        if (G[k].valid) first = k;
+      if (first < 0) continue;
+      int rel[kSpreadGroup][3], lo[3], ext[3];
+      bool fits = K >= kSpreadWin;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        int mn = 0, mx = 0;
+#pragma unroll
+        for (int k = 0; k < kSpreadGroup; ++k) {
+          int v = G[k].org[d] - G[first].org[d];
+          v %= K;
+          if (v > K / 2) v -= K;
+          if (v <= -((K + 1) / 2)) v += K;
+          rel[k][d] = v;
+          if (G[k].valid) {
+            mn = min(mn, v);
+            mx = max(mx, v);
+          }
+        }
+        lo[d] = mn;
+        ext[d] = mx - mn + 6;
+        fits = fits && ext[d] <= kSpreadWin;
+      }
+      if (fits) {
+        // window point (x, y, z) in window coordinates; atom k covers it when
+        // 0 <= x - (rel_k - lo) < 6 on every axis
+        const int rows = ext[0] * ext[1];
+        for (int r = lane; r < rows; r += kWarp) {
+          const int ax = r / ext[1], ay = r % ext[1];
+          float wxy[kSpreadGroup];
+          int oz[kSpreadGroup];
+#pragma unroll
+          for (int k = 0; k < kSpreadGroup; ++k) {
+            const int ix = ax - (rel[k][0] - lo[0]), iy = ay - (rel[k][1] - lo[1]);
+            const bool in = G[k].valid && ix >= 0 && ix < 6 && iy >= 0 && iy < 6;
+            wxy[k] = in ? G[k].q * G[k].w[0][ix] * G[k].w[1][iy] : 0.f;
+            oz[k] = in ? rel[k][2] - lo[2] : 1 << 20;  // outside every z
+          }
+          int gx = (G[first].org[0] + lo[0] + ax) % K, gy = (G[first].org[1] + lo[1] + ay) % K;
+          gx += gx < 0 ? K : 0;
+          gy += gy < 0 ? K : 0;
+          const int64_t row = ((int64_t)gx * K + gy) * K;
+          int gz = (G[first].org[2] + lo[2]) % K;
+          gz += gz < 0 ? K : 0;
+          for (int z = 0; z < ext[2]; ++z) {
+            unsigned long long acc = 0ull;
+            bool any = false;
+#pragma unroll
+            for (int k = 0; k < kSpreadGroup; ++k) {
+              const int iz = z - oz[k];
+              if (iz >= 0 && iz < 6) {
+                acc += to_fix((double)(wxy[k] * G[k].w[2][iz]));
+                any = true;
+              }
+            }
+            if (any) atomicAdd(&grid[row + gz], acc);
+            gz = (gz + 1 == K) ? 0 : gz + 1;
+          }
+        }
+      } else {
+        // atom by atom: lanes over the 36 (x, y) rows, 6 z points each
+#pragma unroll 1
+        for (int k = 0; k < kSpreadGroup; ++k) {
+          const GroupStencil &g = G[k];
+          if (!g.valid) continue;
+          for (int r = lane; r < 36; r += kWarp) {
+            const int a = r / 6, b = r % 6;
+            int gx = (g.org[0] + a) % K, gy = (g.org[1] + b) % K, gz = g.org[2] % K;
+            gx += gx < 0 ? K : 0;
+            gy += gy < 0 ? K : 0;
+            gz += gz < 0 ? K : 0;
+            const float wxy = g.q * g.w[0][a] * g.w[1][b];
+            const int64_t row = ((int64_t)gx * K + gy) * K;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+              atomicAdd(&grid[row + gz], to_fix((double)(wxy * g.w[2][c])));
+              gz = (gz + 1 == K) ? 0 : gz + 1;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+template <class Atoms>
+__global__ void __launch_bounds__(kPmeBlock) pme_spread_grouped_kernel(Atoms atoms, int64_t n, const float *box, int K,
+                                                                       unsigned long long *grid) {
+  __shared__ PmeShared sh;
+  __shared__ GroupStencil st[kPmeBlock / kWarp][kSpreadGroup * kGroupsPerPass];
+  if (threadIdx.x == 0) load_pme_shared(box, K, sh);
+  __syncthreads();
+  spread_groups(atoms, n, sh, K, grid, blockIdx.x, gridDim.x, st[threadIdx.x >> 5]);
 }
 
 template <class T, class Atoms>
@@ -646,12 +805,16 @@ static __global__ void batch_fix_to_real_kernel(const BatchShape *shape, const u
 // the inner loops' register allocation).
 template <class T>
 __device__ __noinline__ void batch_spread_unit(const BatchSys *sys, const T *x, const T *q, const T *boxes,
-                                               typename Acc<T>::S *grid, int sy, int bx, PmeShared &sh) {
+                                               typename Acc<T>::S *grid, int sy, int bx, PmeShared &sh,
+                                               GroupStencil *st) {
   const BatchSys &b = sys[sy];
   if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
   __syncthreads();
   PlainAtoms<T> atoms{x + 3 * b.atom_off, q + b.atom_off, b.natoms};
-  spread_atoms<T>(atoms, b.natoms, sh, b.K, grid + b.grid_off, bx, b.pme_blocks);
+  if constexpr (sizeof(T) == 4)
+    spread_groups(atoms, b.natoms, sh, b.K, grid + b.grid_off, bx, b.pme_blocks, st);
+  else
+    spread_atoms<T>(atoms, b.natoms, sh, b.K, grid + b.grid_off, bx, b.pme_blocks);
 }
 
 template <class T>
@@ -659,10 +822,12 @@ __global__ void __launch_bounds__(kPmeBlock, 4) batch_spread_kernel(const BatchS
                                                                  const T *x, const T *q, const T *boxes,
                                                                  typename Acc<T>::S *grid, unsigned *counter) {
   __shared__ PmeShared sh;
+  __shared__ GroupStencil st[sizeof(T) == 4 ? kPmeBlock / kWarp : 1][kSpreadGroup * kGroupsPerPass];
   const int nsys = shape->nsys, units = shape->pb_units;
   for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
     const int sy = unit_system<false>(sys, nsys, u);
-    batch_spread_unit<T>(sys, x, q, boxes, grid, sy, u - sys[sy].pb_off, sh);
+    batch_spread_unit<T>(sys, x, q, boxes, grid, sy, u - sys[sy].pb_off, sh,
+                         st[sizeof(T) == 4 ? threadIdx.x >> 5 : 0]);
   }
 }
 
@@ -815,9 +980,18 @@ int pme_grid_phase(const PmePlanImpl &p, const PmeLayout &L, char *ws, Atoms ato
   TFF_CUDA(cudaMemsetAsync(ws + L.zero_off, 0, L.zero_bytes, s));
   S *grid = reinterpret_cast<S *>(ws + L.fix);
   if (nthreads > 0) {
-    const int64_t lanes = nthreads * kLanesPerAtom;
-    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((lanes + kPmeBlock - 1) / kPmeBlock, sm_count() * 8));
-    pme_spread_kernel<T, Atoms><<<nb, kPmeBlock, 0, s>>>(atoms, nthreads, box, p.K, grid);
+    if constexpr (sizeof(T) == 4 && std::is_same<Atoms, PlainAtoms<float>>::value) {
+      // FP32 caller-order atoms: groups of consecutive atoms (bit-identical grid), one warp
+      // per group up to a few waves of blocks
+      const int64_t groups = (nthreads + kSpreadGroup - 1) / kSpreadGroup;
+      const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((groups * kWarp + kPmeBlock - 1) / kPmeBlock,
+                                                                 sm_count() * 8));
+      pme_spread_grouped_kernel<Atoms><<<nb, kPmeBlock, 0, s>>>(atoms, nthreads, box, p.K, grid);
+    } else {
+      const int64_t lanes = nthreads * kLanesPerAtom;
+      const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((lanes + kPmeBlock - 1) / kPmeBlock, sm_count() * 8));
+      pme_spread_kernel<T, Atoms><<<nb, kPmeBlock, 0, s>>>(atoms, nthreads, box, p.K, grid);
+    }
     TFF_LAUNCHED();
   }
   return pme_solve_phase<T>(p, L, ws, box, alpha, xmod, ymod, zmod, s, phi_grid);
