@@ -36,10 +36,11 @@ def lib_path() -> str:
     return os.path.join(PKG_DIR, LIB_NAME)
 
 
-# TorchScript binding for C++ hosts (torch.classes.torchff_b200.System), linked against
-# libtffb200.so and libtorch; built with the host C++ compiler.
+# libtorch binding for C++ hosts and the Python package alike, linked against libtffb200.so
+# and libtorch, built with the host C++ compiler: the drop-in torch.ops.torchff.* operators
+# (torch_ops.cpp) and the TorchScript class torch.classes.torchff_b200.System (torch_shim.cpp).
 TORCH_LIB_NAME = "libtffb200_torch.so"
-TORCH_SHIM = "torch_shim.cpp"
+TORCH_SOURCES = ["torch_ops.cpp", "torch_shim.cpp"]
 
 
 def torch_lib_path() -> str:
@@ -49,9 +50,9 @@ def torch_lib_path() -> str:
 def build_torch_shim(force: bool = False) -> str:
     import torch.utils.cpp_extension as ce
 
-    src = os.path.join(CSRC, TORCH_SHIM)
+    srcs = [os.path.join(CSRC, f) for f in TORCH_SOURCES]
     out = torch_lib_path()
-    deps = [src, os.path.join(INCLUDE, "tffb200.h"), lib_path()]
+    deps = [*srcs, os.path.join(INCLUDE, "tffb200.h"), lib_path()]
     if not force and os.path.exists(out) and not _needs_rebuild(out, deps):
         return out
     import torch
@@ -61,7 +62,7 @@ def build_torch_shim(force: bool = False) -> str:
     cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", "-fPIC", "-shared",
            f"-D_GLIBCXX_USE_CXX11_ABI={int(torch._C._GLIBCXX_USE_CXX11_ABI)}",
            *[f"-I{p}" for p in ce.include_paths()], f"-I{os.path.join(cuda, 'include')}", f"-I{INCLUDE}",
-           src, "-o", out, f"-L{tlib}", "-ltorch", "-ltorch_cpu", "-lc10", "-lc10_cuda", f"-L{PKG_DIR}", "-ltffb200",
+           *srcs, "-o", out, f"-L{tlib}", "-ltorch", "-ltorch_cpu", "-lc10", "-lc10_cuda", f"-L{PKG_DIR}", "-ltffb200",
            "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{tlib}"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
