@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section of the water3000 line")
+    ap.add_argument("--no-large-box", action="store_true",
+                    help="skip the 100,000-water section (large_box) of the water3000 line")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 timing of the water3000 line")
     ap.add_argument("--serving-requests", type=int, default=4096)
     ap.add_argument("--no-force-matching", action="store_true", help="skip the force-matching section")
@@ -140,8 +142,9 @@ class ClockSampler:
 # our implementation
 # ---------------------------------------------------------------------------------------
 
-def count_pairs(wb, dtype, device):
-    """In-cutoff half pairs (exclusions removed) of the frame: the algorithmic pair count."""
+def count_pairs(wb, dtype, device, max_npairs: int | None = None):
+    """In-cutoff half pairs (exclusions removed) of the frame: the algorithmic pair count (the
+    cell list counts every pair it finds, also beyond a short max_npairs)."""
     import torch
 
     import torchff_b200  # noqa: F401
@@ -150,7 +153,7 @@ def count_pairs(wb, dtype, device):
     rp, col = (t.to(device) for t in convert_pairs_coo_to_csr(torch.tensor(wb.nblist_exclusions), wb.natoms))
     x = torch.tensor(wb.coords, dtype=torch.float64, device=device)
     b = torch.tensor(wb.box, dtype=torch.float64, device=device)
-    cap = int(wb.natoms * 4 / 3 * math.pi * wb.cutoff ** 3 * 100 / 2 * 1.5)
+    cap = int(wb.natoms * 4 / 3 * math.pi * wb.cutoff ** 3 * 100 / 2 * 1.5) if max_npairs is None else max_npairs
     _, n = torch.ops.torchff.build_neighbor_list_cell_list(x, b, wb.cutoff, cap, rp, col, False)
     return int(n.item())
 
@@ -286,6 +289,79 @@ def time_graph_evals(wb, dtype, device, steps: int, warmup: int) -> dict:
     return {"value": round(steps / (total / 1e3), 2), "unit": "evals/s", "ms_per_step": round(total / steps, 5),
             "steps": steps, "warmup": warmup,
             "_result": (float(energy.item()), forces.double().cpu().numpy())}
+
+
+def time_large_box(device, steps: int = 100, warmup: int = 5) -> dict:
+    """The 100,000-water box (300,000 atoms, mixed precision) in the default line: evals/s by
+    CUDA-graph replays with an L2 flush in between, the stage times, and the pair kernel's
+    roofline at this size (its achieved FP32 rate over the mean pair-stage time)."""
+    import torch
+
+    from torchff_b200.system import FixedChargeSystem, StageTimer
+
+    wb = water_box("water100k", 0)
+    dtype = torch.float32
+    system = FixedChargeSystem.from_water_box(wb, dtype=dtype, device=device)
+    x = torch.tensor(wb.coords, dtype=dtype, device=device)
+    b = torch.tensor(wb.box, dtype=dtype, device=device)
+    energy = torch.empty(1, dtype=torch.float64, device=device)
+    forces = torch.empty_like(x)
+    timer = StageTimer()
+    side = torch.cuda.Stream(device)
+    side.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            system.evaluate_timed_into(x, b, energy, forces, timer)
+            system.evaluate_into(x, b, energy, forces)
+    torch.cuda.current_stream(device).wait_stream(side)
+    torch.cuda.synchronize(device)
+    if system.status() != 0:
+        raise RuntimeError("cluster neighbour list overflow")
+    graph, tgraph = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        system.evaluate_into(x, b, energy, forces)
+    with torch.cuda.graph(tgraph):
+        system.evaluate_timed_into(x, b, energy, forces, timer)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i in range(warmup):
+        flush.fill_(i & 0xff)
+        graph.replay()
+    total = 0.0
+    for i in range(steps):
+        flush.fill_(i & 0xff)
+        start.record()
+        graph.replay()
+        end.record()
+        end.synchronize()
+        total += start.elapsed_time(end)
+    n_stage = min(steps, 50)
+    acc = {k: 0.0 for k in StageTimer.STAGES}
+    for i in range(n_stage):
+        flush.fill_(i & 0xff)
+        tgraph.replay()
+        torch.cuda.synchronize(device)
+        for k, v in timer.stages_ms().items():
+            acc[k] += v
+    del graph, tgraph
+    stages = {k: round(v / n_stage * 1e3, 2) for k, v in acc.items()}
+    npairs = count_pairs(wb, dtype, device, max_npairs=1)
+    sm_max = float(measured_peaks().get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
+    achieved = 60.0 * npairs / (stages["tile_kernel"] * 1e-6) / 1e12
+    traffic = ncu_traffic("pair_tile_kernel", "water100k")
+    issue = ncu_traffic("pair_tile_kernel", "water100k", "ncu_issue.txt")
+    return {"workload": f"water100k: {WORKLOAD_TEXT['water100k']}", "precision": "mixed",
+            "value": round(steps / (total / 1e3), 2), "unit": "evals/s", "ms_per_step": round(total / steps, 4),
+            "steps": steps, "warmup": warmup, "l2": "flushed between timed steps (256 MiB device write)",
+            "stage_us_mean": stages,
+            "roofline": {"kernel": "pair_tile_kernel<float>", "bound": "fp32", "achieved": round(achieved, 4),
+                         "peak": round(fp32_peak, 2), "unit": "TFLOP/s", "frac": round(achieved / fp32_peak, 5),
+                         "traffic": traffic["value"], "traffic_source": traffic, "issue_active": issue["value"],
+                         "algorithmic": f"60 flop x {npairs} in-cutoff pairs per launch / mean pair-stage time "
+                                        f"{stages['tile_kernel']:.1f} us (CUDA events in the graph)"},
+            "throughput": {"pairs_per_s": round(npairs * steps / (total / 1e3)),
+                           "unit": "in-cutoff pairs per second, each pair once"}}
 
 
 def run_force_matching(device, dtype, rank: int, world: int, frames: int = 16, steps: int = 10,
@@ -709,6 +785,8 @@ def run_ours(args):
         if world == 1 and not args.no_fp64 and dtype == torch.float32:
             result["fp64"] = time_graph_evals(wb, torch.float64, device, min(args.steps, 500), args.warmup)
             fp64_result = result["fp64"].pop("_result")
+        if world == 1 and not args.no_large_box and args.workload == "water3000":
+            result["large_box"] = time_large_box(device)
         if world == 1 and not args.no_serving:
             result["serving"] = run_serving(device, args.serving_requests)
         oracle_ref = None
@@ -737,7 +815,7 @@ def run_ours(args):
         result["clocks"] = clocks.summary()
         result["clocks_whole_run"] = dict(clocks.summary((run_t0, datetime.datetime.now())), note=(
             "nvidia-smi samples over the whole run of this line (timed steps, stage timing, e2e, force matching, "
-            "FP64, serving, reference GPU): the timed steps alone can be shorter than one 50 ms sample"))
+            "FP64, large box, serving, reference GPU): the timed steps alone can be shorter than one 50 ms sample"))
     else:
         clocks.stop()
     del graph
