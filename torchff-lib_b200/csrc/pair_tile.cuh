@@ -59,20 +59,25 @@ struct PairTileSmem {
 // the lane's i atoms (the j force is its negative) and the k-free charge gradient.
 template <class T> struct JSums { typename P2T<T>::type fx, fy, fz, dq; };
 
-// Two pairs (i; j0, j1): LJ + erfc-screened Coulomb. dx, dy, dz = r_i - r_j (paired), with
-// r2 = dx^2, then + dy^2, then + dz^2 by fused multiply-adds (the order box_gap2 repeats);
-// ok0 / ok1: the pair may contribute (valid, not excluded, counted by this side). Charge
-// gradients are accumulated k-free (times k when added).
-__device__ __forceinline__ void pair2_eval(float2 dx, float2 dy, float2 dz, bool ok0, bool ok1, float qi, float kqi,
-                                           float sgi, float epi, float2 qj, float2 sgj, float2 epj, float rc2,
+// Squared distances of two pairs: dx^2, then + dy^2, then + dz^2 by fused multiply-adds
+// (the order box_gap2 repeats).
+template <class P2>
+__device__ __forceinline__ P2 pair2_r2(P2 dx, P2 dy, P2 dz) {
+  P2 r2 = p_mul(dx, dx);
+  r2 = p_fma(dy, dy, r2);
+  return p_fma(dz, dz, r2);
+}
+
+// Two pairs (i; j0, j1): LJ + erfc-screened Coulomb. dx, dy, dz = r_i - r_j (paired), r2
+// from pair2_r2; in0 / in1: the pair contributes (valid, not excluded, counted by this
+// side, r2 <= rc2). Charge gradients are accumulated k-free (times k when added).
+__device__ __forceinline__ void pair2_eval(float2 dx, float2 dy, float2 dz, float2 r2, bool in0, bool in1, float qi,
+                                           float kqi, float sgi, float epi, float2 qj, float2 sgj, float2 epj,
                                            float alpha, float two_a_rpi, float &fxi, float &fyi, float &fzi,
                                            float &dqi, JSums<float> &js, float2 &te) {
   const float2 one2 = p_splat(1.f), mone2 = p_splat(-1.f);
-  float2 r2 = p_mul(dx, dx);
-  r2 = p_fma(dy, dy, r2);
-  r2 = p_fma(dz, dz, r2);
   // pairs outside the cutoff (or masked) get rinv = 0, which zeroes every term below
-  const float2 rinv = make_float2((ok0 && r2.x <= rc2) ? rsqrtf(r2.x) : 0.f, (ok1 && r2.y <= rc2) ? rsqrtf(r2.y) : 0.f);
+  const float2 rinv = make_float2(in0 ? rsqrtf(r2.x) : 0.f, in1 ? rsqrtf(r2.y) : 0.f);
   const float2 rinv2 = p_mul(rinv, rinv);
   const float2 u = p_mul(p_mul(r2, rinv), p_splat(alpha));
   // erfc(u) exp(u^2) by Abramowitz & Stegun 7.1.26 (see erfc_exp_as)
@@ -108,21 +113,20 @@ __device__ __forceinline__ void pair2_eval(float2 dx, float2 dy, float2 dz, bool
   te = p_fma(p_mul(es6, p_splat(4.f)), p_add(sr6, mone2), te);
 }
 
-__device__ __forceinline__ void pair2_eval(D2 dx, D2 dy, D2 dz, bool ok0, bool ok1, double qi, double kqi, double sgi,
-                                           double epi, D2 qj, D2 sgj, D2 epj, double rc2, double alpha,
+__device__ __forceinline__ void pair2_eval(D2 dx, D2 dy, D2 dz, D2 r2p, bool in0, bool in1, double qi, double kqi,
+                                           double sgi, double epi, D2 qj, D2 sgj, D2 epj, double alpha,
                                            double two_a_rpi, double &fxi, double &fyi, double &fzi, double &dqi,
                                            JSums<double> &js, D2 &te) {
   const double ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
   const double qq[2] = {qj.x, qj.y}, ss[2] = {sgj.x, sgj.y}, ee[2] = {epj.x, epj.y};
-  const bool ok[2] = {ok0, ok1};
+  const double rr[2] = {r2p.x, r2p.y};
+  const bool in[2] = {in0, in1};
   double jfx[2], jfy[2], jfz[2], jdq[2], e[2];
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
     jfx[k] = jfy[k] = jfz[k] = jdq[k] = e[k] = 0.0;
-    double r2 = ddx[k] * ddx[k];
-    r2 = fma(ddy[k], ddy[k], r2);
-    r2 = fma(ddz[k], ddz[k], r2);
-    if (ok[k] && r2 <= rc2) {
+    const double r2 = rr[k];
+    if (in[k]) {
       const double rinv = rsqrt(r2);
       const double rinv2 = rinv * rinv;
       const double u = alpha * (r2 * rinv);
@@ -407,7 +411,12 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
             ok0 = ok0 && !((xm[c] >> j0) & 1u) && (!diag || j0 < il);
             ok1 = ok1 && !((xm[c] >> j1) & 1u) && (!diag || j1 < il);
           }
-          pair2_eval(dx, dy, dz, ok0, ok1, pi.w, kc * pi.w, li.x, li.y, qj, sgj, epj, rc2, alpha, two_a_rpi,
+          const P2 r2 = pair2_r2(dx, dy, dz);
+          const bool in0 = ok0 && r2.x <= rc2, in1 = ok1 && r2.y <= rc2;
+          // a quarter of the screened-in sub-tiles hold no pair within the cutoff (3000-water
+          // box): the warp skips their arithmetic together
+          if (!__any_sync(kFull, in0 || in1)) continue;
+          pair2_eval(dx, dy, dz, r2, in0, in1, pi.w, kc * pi.w, li.x, li.y, qj, sgj, epj, alpha, two_a_rpi,
                      fx[c], fy[c], fz[c], dq[c], js, te);
         }
         // j side (dE/dx_j = -sum over i of (dE/dr)/r (r_i - r_j)): reduce-scatter over the 8
