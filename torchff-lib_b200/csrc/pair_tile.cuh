@@ -388,6 +388,7 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
         const bool vj0 = (jvalid >> j0) & 1u, vj1 = (jvalid >> j1) & 1u;
         JSums<T> js;
         js.fx = js.fy = js.fz = js.dq = p_splat(T(0));
+        bool hit = false;  // some sub-tile of cj holds a pair within the cutoff (warp-uniform)
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           if (!((col >> c) & 1u)) continue;
@@ -416,9 +417,11 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
           // a quarter of the screened-in sub-tiles hold no pair within the cutoff (3000-water
           // box): the warp skips their arithmetic together
           if (!__any_sync(kFull, in0 || in1)) continue;
+          hit = true;
           pair2_eval(dx, dy, dz, r2, in0, in1, pi.w, kc * pi.w, li.x, li.y, qj, sgj, epj, alpha, two_a_rpi,
                      fx[c], fy[c], fz[c], dq[c], js, te);
         }
+        if (!hit) continue;  // nothing to add for cj (a sixth of the screened-in cj at 3000 waters)
         // j side (dE/dx_j = -sum over i of (dE/dr)/r (r_i - r_j)): reduce-scatter over the 8
         // lanes ti that hold j0, j1; lane ti ends with value ti (j0: x y z q, j1: x y z q)
         T v[8] = {-js.fx.x, -js.fy.x, -js.fz.x, js.dq.x, -js.fx.y, -js.fy.y, -js.fz.y, js.dq.y};
