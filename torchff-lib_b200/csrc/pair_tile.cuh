@@ -43,15 +43,21 @@ __device__ __forceinline__ D2 p_mul(D2 a, D2 b) { return D2{a.x * b.x, a.y * b.y
 __device__ __forceinline__ D2 p_fma(D2 a, D2 b, D2 c) { return D2{fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)}; }
 __device__ __forceinline__ D2 p_splat(double a) { return D2{a, a}; }
 
-// Per-warp staging: cluster J's positions (moved to the pair's image; padding slots far
-// away) with the charge in w and LJ parameters (sigma/2, sqrt eps); the same for cluster I
-// (padding far the other way), and I's four sub-cluster boxes (lo xyz, hi xyz).
+// Per-warp staging, laid out as the paired operands the arithmetic takes, so that one
+// 16-byte shared load gives two of them:
+// - cluster J (moved to the pair's image; padding slots far away): jp[w][k][4 cj + tj]
+//   holds the two j atoms j0 = 8 cj + tj and j1 = j0 + 4 of lane column tj,
+//   k = 0: (-x0, -x1, -y0, -y1), 1: (-z0, -z1, q0, q1), 2: (s0, s1, e0, e1), with s = sigma/2
+//   and e = sqrt(eps);
+// - cluster I (padding far the other way), each value doubled: ip[w][k][atom],
+//   k = 0: (x, x, y, y), 1: (z, z, q, q), 2: (s, s, e, e), 3: (kq, kq, -kq, -kq);
+// - I's four sub-cluster boxes (lo xyz, hi xyz).
+// Entries are indexed by atom (I) or lane column (J) innermost, so the 8 (4) distinct
+// entries a warp reads at once are contiguous: one shared-memory wavefront.
 template <class T, int NW>
 struct PairTileSmem {
-  typename V4<T>::type pos[NW][kWarp];
-  typename V2<T>::type lj[NW][kWarp];
-  typename V4<T>::type ipos[NW][kWarp];
-  typename V2<T>::type ilj[NW][kWarp];
+  typename V4<T>::type jp[NW][3][16];
+  typename V4<T>::type ip[NW][4][kWarp];
   T ibox[NW][4][6];
 };
 
@@ -71,10 +77,11 @@ __device__ __forceinline__ P2 pair2_r2(P2 dx, P2 dy, P2 dz) {
 // Two pairs (i; j0, j1): LJ + erfc-screened Coulomb. dx, dy, dz = r_i - r_j (paired), r2
 // from pair2_r2; in0 / in1: the pair contributes (valid, not excluded, counted by this
 // side, r2 <= rc2). Charge gradients are accumulated k-free (times k when added).
-__device__ __forceinline__ void pair2_eval(float2 dx, float2 dy, float2 dz, float2 r2, bool in0, bool in1, float qi,
-                                           float kqi, float sgi, float epi, float2 qj, float2 sgj, float2 epj,
-                                           float alpha, float two_a_rpi, float &fxi, float &fyi, float &fzi,
-                                           float &dqi, JSums<float> &js, float2 &te) {
+// The i-side operands come doubled: qi2 = (q_i, q_i), kqi2 = k q_i, nkqi2 = -k q_i, sgi2, epi2.
+__device__ __forceinline__ void pair2_eval(float2 dx, float2 dy, float2 dz, float2 r2, bool in0, bool in1, float2 qi2,
+                                           float2 kqi2, float2 nkqi2, float2 sgi2, float2 epi2, float2 qj,
+                                           float2 sgj, float2 epj, float alpha, float two_a_rpi, float &fxi,
+                                           float &fyi, float &fzi, float &dqi, JSums<float> &js, float2 &te) {
   const float2 one2 = p_splat(1.f), mone2 = p_splat(-1.f);
   // pairs outside the cutoff (or masked) get rinv = 0, which zeroes every term below
   const float2 rinv = make_float2(in0 ? rsqrtf(r2.x) : 0.f, in1 ? rsqrtf(r2.y) : 0.f);
@@ -94,9 +101,9 @@ __device__ __forceinline__ void pair2_eval(float2 dx, float2 dy, float2 dz, floa
   const float2 ecr = p_mul(ec, rinv);  // erfc(u) / r
   const float2 cq = p_mul(qj, ecr);    // E_coul / (k q_i)
   const float2 g = p_fma(p_splat(two_a_rpi), p_mul(ex, rinv), p_mul(ec, rinv2));
-  float2 dedr = p_mul(p_mul(g, rinv), p_mul(qj, p_splat(-kqi)));  // (dE/dr) / r, Coulomb
-  const float2 sig = p_add(p_splat(sgi), sgj);
-  const float2 eps = p_mul(p_splat(epi), epj);
+  float2 dedr = p_mul(p_mul(g, rinv), p_mul(qj, nkqi2));  // (dE/dr) / r, Coulomb
+  const float2 sig = p_add(sgi2, sgj);
+  const float2 eps = p_mul(epi2, epj);
   const float2 sr2 = p_mul(p_mul(sig, sig), rinv2);
   const float2 sr6 = p_mul(p_mul(sr2, sr2), sr2);
   const float2 es6 = p_mul(eps, sr6);
@@ -108,15 +115,17 @@ __device__ __forceinline__ void pair2_eval(float2 dx, float2 dy, float2 dz, floa
   js.fx = p_fma(dedr, dx, js.fx);
   js.fy = p_fma(dedr, dy, js.fy);
   js.fz = p_fma(dedr, dz, js.fz);
-  js.dq = p_fma(p_splat(qi), ecr, js.dq);
-  te = p_fma(cq, p_splat(kqi), te);
+  js.dq = p_fma(qi2, ecr, js.dq);
+  te = p_fma(cq, kqi2, te);
   te = p_fma(p_mul(es6, p_splat(4.f)), p_add(sr6, mone2), te);
 }
 
-__device__ __forceinline__ void pair2_eval(D2 dx, D2 dy, D2 dz, D2 r2p, bool in0, bool in1, double qi, double kqi,
-                                           double sgi, double epi, D2 qj, D2 sgj, D2 epj, double alpha,
+__device__ __forceinline__ void pair2_eval(D2 dx, D2 dy, D2 dz, D2 r2p, bool in0, bool in1, D2 qi2, D2 kqi2,
+                                           D2 nkqi2, D2 sgi2, D2 epi2, D2 qj, D2 sgj, D2 epj, double alpha,
                                            double two_a_rpi, double &fxi, double &fyi, double &fzi, double &dqi,
                                            JSums<double> &js, D2 &te) {
+  const double qi = qi2.x, kqi = kqi2.x, sgi = sgi2.x, epi = epi2.x;
+  (void)nkqi2;
   const double ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
   const double qq[2] = {qj.x, qj.y}, ss[2] = {sgj.x, sgj.y}, ee[2] = {epj.x, epj.y};
   const double rr[2] = {r2p.x, r2p.y};
@@ -266,9 +275,13 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
       T lo[3], hi[3];
       subcluster_box<T>(vl, p.x, p.y, p.z, lo, hi);
       if (!vl) p.x = p.y = p.z = -far;
+      const W2 l = A.lj[sl];
+      const T kq = kc * p.w;
       __syncwarp();  // every lane is done with the previous item's staging
-      sm.ipos[w][lane] = p;
-      sm.ilj[w][lane] = A.lj[sl];
+      sm.ip[w][0][lane] = make_v4(p.x, p.x, p.y, p.y);
+      sm.ip[w][1][lane] = make_v4(p.z, p.z, p.w, p.w);
+      sm.ip[w][2][lane] = make_v4(l.x, l.x, l.y, l.y);
+      sm.ip[w][3][lane] = make_v4(kq, kq, -kq, -kq);
       if (ti == 0) {
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
@@ -339,9 +352,20 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
         pj.w = T(0);
       }
       const unsigned jvalid = __ballot_sync(kFull, vj);
+      const W2 lj = A.lj[sJ + lane];
       __syncwarp();  // every lane is done with the previous J's staging
-      sm.pos[w][lane] = pj;
-      sm.lj[w][lane] = A.lj[sJ + lane];
+      {
+        // atom lane = 8 cj + tj + 4 h goes to entry 4 cj + tj, slot h of each pair
+        T *e0 = reinterpret_cast<T *>(&sm.jp[w][0][4 * (lane >> 3) + (lane & 3)]) + ((lane >> 2) & 1);
+        T *e1 = reinterpret_cast<T *>(&sm.jp[w][1][4 * (lane >> 3) + (lane & 3)]) + ((lane >> 2) & 1);
+        T *e2 = reinterpret_cast<T *>(&sm.jp[w][2][4 * (lane >> 3) + (lane & 3)]) + ((lane >> 2) & 1);
+        e0[0] = -pj.x;
+        e0[2] = -pj.y;
+        e1[0] = -pj.z;
+        e1[2] = pj.w;
+        e2[0] = lj.x;
+        e2[2] = lj.y;
+      }
       // active sub-tiles: bit ci + 4 cj. Without a common shift every sub-tile is taken.
       unsigned act = 0xffffu;
       if (shifted) {
@@ -381,10 +405,9 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
         const unsigned col = (act >> (4 * cj)) & 0xfu;  // i sub-clusters active against cj
         if (!col) continue;
         const int j0 = 8 * cj + tj, j1 = j0 + 4;
-        const V a0 = sm.pos[w][j0], a1 = sm.pos[w][j1];
-        const W2 l0 = sm.lj[w][j0], l1 = sm.lj[w][j1];
-        const P2 nxj = P2{-a0.x, -a1.x}, nyj = P2{-a0.y, -a1.y}, nzj = P2{-a0.z, -a1.z};
-        const P2 qj = P2{a0.w, a1.w}, sgj = P2{l0.x, l1.x}, epj = P2{l0.y, l1.y};
+        const V ja = sm.jp[w][0][4 * cj + tj], jb = sm.jp[w][1][4 * cj + tj], jc = sm.jp[w][2][4 * cj + tj];
+        const P2 nxj = P2{ja.x, ja.y}, nyj = P2{ja.z, ja.w}, nzj = P2{jb.x, jb.y};
+        const P2 qj = P2{jb.z, jb.w}, sgj = P2{jc.x, jc.y}, epj = P2{jc.z, jc.w};
         const bool vj0 = (jvalid >> j0) & 1u, vj1 = (jvalid >> j1) & 1u;
         JSums<T> js;
         js.fx = js.fy = js.fz = js.dq = p_splat(T(0));
@@ -392,11 +415,10 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           if (!((col >> c) & 1u)) continue;
-          const V pi = sm.ipos[w][8 * c + ti];
-          const W2 li = sm.ilj[w][8 * c + ti];
-          P2 dx = p_add(p_splat(pi.x), nxj);
-          P2 dy = p_add(p_splat(pi.y), nyj);
-          P2 dz = p_add(p_splat(pi.z), nzj);
+          const V ia = sm.ip[w][0][8 * c + ti], ib = sm.ip[w][1][8 * c + ti];
+          P2 dx = p_add(P2{ia.x, ia.y}, nxj);
+          P2 dy = p_add(P2{ia.z, ia.w}, nyj);
+          P2 dz = p_add(P2{ib.x, ib.y}, nzj);
           const bool vi = (ivalid >> (8 * c + ti)) & 1u;
           bool ok0 = vi, ok1 = vi;
           if (!shifted) {
@@ -418,8 +440,9 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
           // box): the warp skips their arithmetic together
           if (!__any_sync(kFull, in0 || in1)) continue;
           hit = true;
-          pair2_eval(dx, dy, dz, r2, in0, in1, pi.w, kc * pi.w, li.x, li.y, qj, sgj, epj, alpha, two_a_rpi,
-                     fx[c], fy[c], fz[c], dq[c], js, te);
+          const V ic = sm.ip[w][2][8 * c + ti], id = sm.ip[w][3][8 * c + ti];
+          pair2_eval(dx, dy, dz, r2, in0, in1, P2{ib.z, ib.w}, P2{id.x, id.y}, P2{id.z, id.w}, P2{ic.x, ic.y},
+                     P2{ic.z, ic.w}, qj, sgj, epj, alpha, two_a_rpi, fx[c], fy[c], fz[c], dq[c], js, te);
         }
         if (!hit) continue;  // nothing to add for cj (a sixth of the screened-in cj at 3000 waters)
         // j side (dE/dx_j = -sum over i of (dE/dr)/r (r_i - r_j)): reduce-scatter over the 8
