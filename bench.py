@@ -811,6 +811,16 @@ def run_ours(args):
                     "device": round(value / rg["value"], 2), "e2e": round(e2e_value / rg["value"], 2),
                     "formula": "this line's value (and e2e value) / reference_gpu.value (the reference's FP64 CUDA "
                                f"ops on the same box and GPU, {rg['fp64']['mode']}, L2 flushed)"}
+            if "large_box" in result:
+                # the same composition of the reference's ops on the 300,000-atom box
+                lb = result["large_box"]
+                rg = reference_gpu_leg(args, "water100k", 20)
+                lb["reference_gpu"] = rg
+                if "value" in rg and rg.get("value"):
+                    lb["speedup_vs_reference_fp64_cuda"] = {
+                        "device": round(lb["value"] / rg["value"], 2),
+                        "formula": "large_box.value / large_box.reference_gpu.value (the reference's FP64 CUDA ops "
+                                   f"on the same 300,000-atom box and GPU, {rg['fp64']['mode']}, L2 flushed)"}
         clocks.stop()
         result["clocks"] = clocks.summary()
         result["clocks_whole_run"] = dict(clocks.summary((run_t0, datetime.datetime.now())), note=(
@@ -982,7 +992,7 @@ def run_reference_gpu(args):
         return
     import glob
 
-    if args.workload not in ("water3000", "water216"):
+    if args.workload not in ("water3000", "water216", "water100k"):
         print(json.dumps({"impl": "reference-gpu", "unavailable": f"no reference GPU run for {args.workload}"}))
         return
     if not glob.glob(os.path.join(REPO, "oracle", "_ref", "*", "*.so")):
@@ -1026,11 +1036,12 @@ def run_reference_gpu(args):
     print(json.dumps(line), flush=True)
 
 
-def reference_gpu_leg(args) -> dict:
+def reference_gpu_leg(args, workload: str | None = None, steps: int | None = None) -> dict:
     """Runs the reference-gpu arm in a child process (after our timed regions) and returns
     its line, or the reason it did not run."""
-    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference-gpu", "--workload", args.workload,
-           "--steps", str(min(max(args.steps, 20), 200)), "--warmup", str(max(args.warmup, 3))]
+    steps = steps if steps is not None else min(max(args.steps, 20), 200)
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference-gpu", "--workload", workload or args.workload,
+           "--steps", str(steps), "--warmup", str(max(args.warmup, 3))]
     env = dict(os.environ)
     for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
         env.pop(k, None)

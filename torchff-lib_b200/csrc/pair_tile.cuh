@@ -419,15 +419,17 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
           P2 dx = p_add(P2{ia.x, ia.y}, nxj);
           P2 dy = p_add(P2{ia.z, ia.w}, nyj);
           P2 dz = p_add(P2{ib.x, ib.y}, nzj);
-          const bool vi = (ivalid >> (8 * c + ti)) & 1u;
-          bool ok0 = vi, ok1 = vi;
+          // with a common shift, padding atoms (I's far one way, J's far the other) lie
+          // outside every cutoff
+          bool ok0 = true, ok1 = true;
           if (!shifted) {
-            // per-pair minimum image; padding j atoms must be masked here (their far
-            // position does not survive the wrap)
+            // per-pair minimum image; padding atoms must be masked here (their far positions
+            // do not survive the wrap)
             pair_min_image(ortho, dx.x, dy.x, dz.x, s_m, s_inv);
             pair_min_image(ortho, dx.y, dy.y, dz.y, s_m, s_inv);
-            ok0 = ok0 && vj0;
-            ok1 = ok1 && vj1;
+            const bool vi = (ivalid >> (8 * c + ti)) & 1u;
+            ok0 = vi && vj0;
+            ok1 = vi && vj1;
           }
           if (special) {
             const int il = 8 * c + ti;
