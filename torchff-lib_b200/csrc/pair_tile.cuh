@@ -1,4 +1,4 @@
-// Real-space energy + forces over HALF cluster lists (each pair evaluated once).
+// FP32 real-space energy + forces over HALF cluster lists (each pair evaluated once).
 //
 // Work item: cluster I (32 atoms, 4 sub-clusters of 8 consecutive atoms along the Hilbert
 // curve) and up to kItemTiles clusters J <= I of its half neighbour list (entries k,
@@ -11,25 +11,26 @@
 //     the same rounding steps as the pair distance, so that a screened-out sub-tile provably
 //     holds no pair within the cutoff;
 //   - for every J sub-cluster with an active sub-tile, lane (ti, tj) takes the two j atoms
-//     8cj + tj and 8cj + tj + 4 as one paired operand (FADD2/FMUL2/FFMA2 in FP32) against
-//     its i atom of each active sub-tile: 64 pairs per sub-tile, each evaluated once;
+//     8cj + tj and 8cj + tj + 4 as one paired operand (FADD2/FMUL2/FFMA2) against its i
+//     atom of each active sub-tile: 64 pairs per sub-tile, each evaluated once; a sub-tile
+//     none of whose pairs lies within the cutoff is skipped after the distances (warp vote);
 //   - the j-side force and charge-gradient sums of the two j atoms are reduce-scattered
 //     over the 8 lanes that hold them (warp shuffles), and each of those lanes adds one of
-//     the 8 sums into the int64 fixed-point (FP32 mode) or FP64 accumulators.
+//     the 8 sums into the int64 fixed-point accumulators.
 // The i-side sums stay in registers for the whole item and are reduce-scattered over the 4
 // lanes of each i atom at its end. Pairs within one cluster (J == I) count j < i; excluded
 // pairs are skipped through a per-J bit mask of each i atom's excluded partners, and their
 // Ewald exclusion correction -k q_i q_j erf(alpha r)/r (r <= rc) is evaluated in FP64 once
 // per excluded pair, by item 0 of the cluster that holds the pair's later slot.
-// Integer accumulation is order-independent, so FP32-mode results are bit-identical run to
-// run; energies are summed per lane in a fixed order and added once per item.
+// Integer accumulation is order-independent, so results are bit-identical run to run;
+// energies are summed per lane in a fixed order and added once per item.
 #pragma once
 
 namespace tff {
 namespace {
 
 // Paired arithmetic on two values: FP32 pairs map onto the packed FP32 instructions of
-// sm_100a; FP64 pairs are two scalar operations.
+// sm_100a (FP64 pairs, two scalar operations, keep the helpers generic).
 template <class T> struct P2T;
 template <> struct P2T<float> { using type = float2; };
 template <> struct P2T<double> { using type = D2; };
@@ -74,40 +75,87 @@ __device__ __forceinline__ P2 pair2_r2(P2 dx, P2 dy, P2 dz) {
   return p_fma(dz, dz, r2);
 }
 
+// Constants of the pair arithmetic, doubled for the paired instructions and passed as a
+// kernel parameter (constant memory) instead of being rebuilt in registers per use.
+// erfc(x) exp(x^2) ~ t (a1 + t (a2 + t (a3 + t (a4 + t a5)))), t = 1 / (1 + p x): Abramowitz &
+// Stegun 7.1.26, |error| <= 1.5e-7.
+template <class T>
+struct PairConst {
+  using P2 = typename P2T<T>::type;
+  P2 one, a1, a2, a3, a4, a5;
+  P2 lj_f1, lj_f0;  // -48, 24: (dE/dr) / r of LJ = eps_ij (sr6) (24 - 48 sr6) / r^2
+  P2 lj_e1, lj_e0;  // 4, -4: E of LJ = eps_ij (sr6) (4 sr6 - 4)
+  P2 alpha_p;       // alpha p
+  P2 nalpha2_log2e; // -alpha^2 log2(e): exp(-(alpha r)^2) = 2^(r^2 (-alpha^2 log2 e))
+  P2 two_a_rpi;     // 2 alpha / sqrt(pi)
+  T alpha;
+};
+
+template <class T>
+PairConst<T> pair_const(double alpha) {
+  using P2 = typename P2T<T>::type;
+  auto d = [](double v) { return P2{(T)v, (T)v}; };
+  PairConst<T> c;
+  c.one = d(1.0);
+  c.a1 = d(0.254829592);
+  c.a2 = d(-0.284496736);
+  c.a3 = d(1.421413741);
+  c.a4 = d(-1.453152027);
+  c.a5 = d(1.061405429);
+  c.lj_f1 = d(-48.0);
+  c.lj_f0 = d(24.0);
+  c.lj_e1 = d(4.0);
+  c.lj_e0 = d(-4.0);
+  c.alpha_p = d(alpha * 0.3275911);
+  c.nalpha2_log2e = d(-alpha * alpha * 1.4426950408889634074);
+  c.two_a_rpi = d(2.0 * alpha / 1.7724538509055160273);
+  c.alpha = (T)alpha;
+  return c;
+}
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Two pairs (i; j0, j1): LJ + erfc-screened Coulomb. dx, dy, dz = r_i - r_j (paired), r2
 // from pair2_r2; in0 / in1: the pair contributes (valid, not excluded, counted by this
 // side, r2 <= rc2). Charge gradients are accumulated k-free (times k when added).
 // The i-side operands come doubled: qi2 = (q_i, q_i), kqi2 = k q_i, nkqi2 = -k q_i, sgi2, epi2.
 __device__ __forceinline__ void pair2_eval(float2 dx, float2 dy, float2 dz, float2 r2, bool in0, bool in1, float2 qi2,
                                            float2 kqi2, float2 nkqi2, float2 sgi2, float2 epi2, float2 qj,
-                                           float2 sgj, float2 epj, float alpha, float two_a_rpi, float &fxi,
+                                           float2 sgj, float2 epj, const PairConst<float> &pc, float &fxi,
                                            float &fyi, float &fzi, float &dqi, JSums<float> &js, float2 &te) {
-  const float2 one2 = p_splat(1.f), mone2 = p_splat(-1.f);
   // pairs outside the cutoff (or masked) get rinv = 0, which zeroes every term below
   const float2 rinv = make_float2(in0 ? rsqrtf(r2.x) : 0.f, in1 ? rsqrtf(r2.y) : 0.f);
   const float2 rinv2 = p_mul(rinv, rinv);
-  const float2 u = p_mul(p_mul(r2, rinv), p_splat(alpha));
-  // erfc(u) exp(u^2) by Abramowitz & Stegun 7.1.26 (see erfc_exp_as)
-  const float2 den = p_fma(u, p_splat(0.3275911f), one2);
-  const float2 tt = make_float2(__fdividef(1.f, den.x), __fdividef(1.f, den.y));
-  float2 poly = p_fma(tt, p_splat(1.061405429f), p_splat(-1.453152027f));
-  poly = p_fma(tt, poly, p_splat(1.421413741f));
-  poly = p_fma(tt, poly, p_splat(-0.284496736f));
-  poly = p_fma(tt, poly, p_splat(0.254829592f));
+  const float2 r = p_mul(r2, rinv);
+  const float2 den = p_fma(r, pc.alpha_p, pc.one);  // 1 + p alpha r
+  const float2 tt = make_float2(rcp_approx(den.x), rcp_approx(den.y));
+  float2 poly = p_fma(tt, pc.a5, pc.a4);
+  poly = p_fma(tt, poly, pc.a3);
+  poly = p_fma(tt, poly, pc.a2);
+  poly = p_fma(tt, poly, pc.a1);
   poly = p_mul(tt, poly);
-  const float2 mu2 = p_mul(u, u);
-  const float2 ex = make_float2(__expf(-mu2.x), __expf(-mu2.y));
-  const float2 ec = p_mul(poly, ex);
-  const float2 ecr = p_mul(ec, rinv);  // erfc(u) / r
+  const float2 xa = p_mul(r2, pc.nalpha2_log2e);
+  const float2 ex = make_float2(ex2_approx(xa.x), ex2_approx(xa.y));  // exp(-(alpha r)^2)
+  const float2 ec = p_mul(poly, ex);   // erfc(alpha r)
+  const float2 ecr = p_mul(ec, rinv);  // erfc(alpha r) / r
   const float2 cq = p_mul(qj, ecr);    // E_coul / (k q_i)
-  const float2 g = p_fma(p_splat(two_a_rpi), p_mul(ex, rinv), p_mul(ec, rinv2));
-  float2 dedr = p_mul(p_mul(g, rinv), p_mul(qj, nkqi2));  // (dE/dr) / r, Coulomb
+  // (dE/dr) / r of the Coulomb term: -k q_i q_j (erfc(alpha r)/r + 2 alpha/sqrt(pi) exp(-(alpha r)^2)) / r^2
+  float2 dedr = p_mul(p_mul(p_fma(pc.two_a_rpi, ex, ecr), rinv2), p_mul(qj, nkqi2));
   const float2 sig = p_add(sgi2, sgj);
   const float2 eps = p_mul(epi2, epj);
   const float2 sr2 = p_mul(p_mul(sig, sig), rinv2);
   const float2 sr6 = p_mul(p_mul(sr2, sr2), sr2);
   const float2 es6 = p_mul(eps, sr6);
-  dedr = p_fma(p_mul(es6, p_splat(-24.f)), p_mul(p_fma(sr6, p_splat(2.f), mone2), rinv2), dedr);
+  dedr = p_fma(p_mul(es6, p_fma(sr6, pc.lj_f1, pc.lj_f0)), rinv2, dedr);
   fxi = fmaf(dedr.x, dx.x, fmaf(dedr.y, dx.y, fxi));
   fyi = fmaf(dedr.x, dy.x, fmaf(dedr.y, dy.y, fyi));
   fzi = fmaf(dedr.x, dz.x, fmaf(dedr.y, dz.y, fzi));
@@ -117,54 +165,7 @@ __device__ __forceinline__ void pair2_eval(float2 dx, float2 dy, float2 dz, floa
   js.fz = p_fma(dedr, dz, js.fz);
   js.dq = p_fma(qi2, ecr, js.dq);
   te = p_fma(cq, kqi2, te);
-  te = p_fma(p_mul(es6, p_splat(4.f)), p_add(sr6, mone2), te);
-}
-
-__device__ __forceinline__ void pair2_eval(D2 dx, D2 dy, D2 dz, D2 r2p, bool in0, bool in1, D2 qi2, D2 kqi2,
-                                           D2 nkqi2, D2 sgi2, D2 epi2, D2 qj, D2 sgj, D2 epj, double alpha,
-                                           double two_a_rpi, double &fxi, double &fyi, double &fzi, double &dqi,
-                                           JSums<double> &js, D2 &te) {
-  const double qi = qi2.x, kqi = kqi2.x, sgi = sgi2.x, epi = epi2.x;
-  (void)nkqi2;
-  const double ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
-  const double qq[2] = {qj.x, qj.y}, ss[2] = {sgj.x, sgj.y}, ee[2] = {epj.x, epj.y};
-  const double rr[2] = {r2p.x, r2p.y};
-  const bool in[2] = {in0, in1};
-  double jfx[2], jfy[2], jfz[2], jdq[2], e[2];
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    jfx[k] = jfy[k] = jfz[k] = jdq[k] = e[k] = 0.0;
-    const double r2 = rr[k];
-    if (in[k]) {
-      const double rinv = rsqrt(r2);
-      const double rinv2 = rinv * rinv;
-      const double u = alpha * (r2 * rinv);
-      double ec, ex;
-      erfc_exp(u, ec, ex);
-      const double ecr = ec * rinv;
-      const double cq = qq[k] * ecr;
-      double dedr = -kqi * qq[k] * (ec * rinv2 + two_a_rpi * ex * rinv) * rinv;
-      const double sig = sgi + ss[k];
-      const double eps = epi * ee[k];
-      const double sr2 = sig * sig * rinv2;
-      const double sr6 = sr2 * sr2 * sr2;
-      dedr -= 24.0 * eps * sr6 * (2.0 * sr6 - 1.0) * rinv2;
-      fxi += dedr * ddx[k];
-      fyi += dedr * ddy[k];
-      fzi += dedr * ddz[k];
-      dqi += cq;
-      jfx[k] = dedr * ddx[k];
-      jfy[k] = dedr * ddy[k];
-      jfz[k] = dedr * ddz[k];
-      jdq[k] = qi * ecr;
-      e[k] = kqi * cq + 4.0 * eps * sr6 * (sr6 - 1.0);
-    }
-  }
-  js.fx = p_add(js.fx, D2{jfx[0], jfx[1]});
-  js.fy = p_add(js.fy, D2{jfy[0], jfy[1]});
-  js.fz = p_add(js.fz, D2{jfz[0], jfz[1]});
-  js.dq = p_add(js.dq, D2{jdq[0], jdq[1]});
-  te = p_add(te, D2{e[0], e[1]});
+  te = p_fma(es6, p_fma(sr6, pc.lj_e1, pc.lj_e0), te);
 }
 
 // Bounding box of each lane's 8-lane group (lanes 8c .. 8c+7 hold sub-cluster c), over
@@ -223,8 +224,10 @@ __device__ __forceinline__ void rs_halve(T (&v)[N], int o, int lane) {
 constexpr int kPairTileWarps = 4;
 template <class T> struct PairTileOcc { static constexpr int min_blocks = sizeof(T) == 4 ? 4 : 3; };
 
+// FP32 only: FP64 real space runs on full lists and tile_kernel (see launch_real_space).
 template <class T, int NW, int MIN_BLOCKS>
-__global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs<T> A) {
+__global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs<T> A, PairConst<T> pc) {
+  static_assert(sizeof(T) == 4, "the pair kernel is the FP32 real-space kernel");
   pdl_enter();
   using V = typename V4<T>::type;
   using W2 = typename V2<T>::type;
@@ -238,9 +241,7 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
   int cur_sys = -1;
   bool ortho = false;
   const T rc2 = (T)(A.rc * A.rc);
-  const T alpha = (T)A.alpha;
   const T kc = (T)A.kc;
-  const T two_a_rpi = (T)(2.0 * A.alpha / 1.7724538509055160273);
   const T far = sizeof(T) == 4 ? T(1e18) : T(1e150);  // padding slots: outside every cutoff
 
   const int nitems = cl.itemoff[cl.n_clusters()];
@@ -444,7 +445,7 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
           hit = true;
           const V ic = sm.ip[w][2][8 * c + ti], id = sm.ip[w][3][8 * c + ti];
           pair2_eval(dx, dy, dz, r2, in0, in1, P2{ib.z, ib.w}, P2{id.x, id.y}, P2{id.z, id.w}, P2{ic.x, ic.y},
-                     P2{ic.z, ic.w}, qj, sgj, epj, alpha, two_a_rpi, fx[c], fy[c], fz[c], dq[c], js, te);
+                     P2{ic.z, ic.w}, qj, sgj, epj, pc, fx[c], fy[c], fz[c], dq[c], js, te);
         }
         if (!hit) continue;  // nothing to add for cj (a sixth of the screened-in cj at 3000 waters)
         // j side (dE/dx_j = -sum over i of (dE/dr)/r (r_i - r_j)): reduce-scatter over the 8
@@ -543,7 +544,8 @@ int launch_real_space(bool pdl, int64_t max_items, int sms, cudaStream_t s, cons
   if constexpr (sizeof(T) == 4) {
     constexpr int NW = kPairTileWarps;
     const int nbt = (int)std::max<int64_t>(1, std::min<int64_t>((max_items + NW - 1) / NW, (int64_t)sms * 48 / NW));
-    return launch_k(pdl, pair_tile_kernel<T, NW, PairTileOcc<T>::min_blocks>, nbt, NW * kWarp, 0, s, A);
+    return launch_k(pdl, pair_tile_kernel<T, NW, PairTileOcc<T>::min_blocks>, nbt, NW * kWarp, 0, s, A,
+                    pair_const<T>(A.alpha));
   } else {
     constexpr int NW = TileCfg<T>::NW;
     const int nbt = (int)std::max<int64_t>(1, std::min<int64_t>((max_items + NW - 1) / NW, (int64_t)sms * 48 / NW));
