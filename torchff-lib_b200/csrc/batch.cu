@@ -50,7 +50,7 @@ struct BatchLayout {
   int cap;
   size_t shape, sys, status, boxinfo, cl_sys, sup_sys, sidx, inv, pos, frac, bc, bh, sbc, sbh, nbr, ncount, itemoff, items;
   size_t lj, exslot, acc, e_tile;
-  size_t fix, real, cplx, partials, tickets, e_pme, pme_grad, pme_phi, moduli;
+  size_t fix, real, cplx, partials, tickets, e_pme, pme_grad, pme_phi, moduli, twiddle;
   size_t bytes;
 };
 
@@ -102,6 +102,7 @@ inline BatchLayout batch_layout(int dtype, int64_t max_atoms, int64_t max_system
   L.pme_grad = take(3 * max_atoms * ts);
   L.pme_phi = take(max_atoms * ts);
   L.moduli = take((size_t)moduli_offset(kBatchMaxK + 1) * ts);
+  L.twiddle = take((size_t)twiddle_offset(kBatchMaxK + 1) * 2 * ts);
   L.bytes = c.bytes();
   return L;
 }
@@ -306,23 +307,24 @@ int batch_enqueue(tff_batch b, int kclass, const T *x, const T *boxes, const T *
     real = reinterpret_cast<T *>(fix);
   }
   auto *cplx = reinterpret_cast<typename CplxOf<T>::type *>(w + L.cplx);
+  const auto *twtab = reinterpret_cast<const typename CplxOf<T>::type *>(w + L.twiddle);
   const size_t dsmem = batch_dft_smem<T>(kclass);
   const int nb_dft = sms * 8;
-  batch_dft_kernel<T, kDftZR2C><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 1);
+  batch_dft_kernel<T, kDftZR2C><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, twtab, counters + 1);
   TFF_LAUNCHED();
-  batch_dft_kernel<T, kDftY><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 2);
+  batch_dft_kernel<T, kDftY><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, twtab, counters + 2);
   TFF_LAUNCHED();
-  batch_dft_kernel<T, kDftX><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 3);
+  batch_dft_kernel<T, kDftX><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, twtab, counters + 3);
   TFF_LAUNCHED();
   batch_convolve_kernel<T><<<nb_pme, kPmeBlock, 0, ps>>>(dsys, shape, cplx, boxes, b->desc.ewald_alpha,
                                                          reinterpret_cast<const T *>(w + L.moduli), partials, tickets,
                                                          e_pme, counters + 4);
   TFF_LAUNCHED();
-  batch_dft_kernel<T, kDftXInv><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 5);
+  batch_dft_kernel<T, kDftXInv><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, twtab, counters + 5);
   TFF_LAUNCHED();
-  batch_dft_kernel<T, kDftYInv><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 6);
+  batch_dft_kernel<T, kDftYInv><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, twtab, counters + 6);
   TFF_LAUNCHED();
-  batch_dft_kernel<T, kDftZC2R><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, counters + 7);
+  batch_dft_kernel<T, kDftZC2R><<<nb_dft, kDftThreads, dsmem, ps>>>(dsys, shape, real, cplx, twtab, counters + 7);
   TFF_LAUNCHED();
 
   // --- real space on the caller stream
@@ -515,6 +517,17 @@ int tff_batch_create(const tff_batch_desc *desc, tff_batch *out) {
       std::vector<float> mf(mod.begin(), mod.end());
       e = cudaMemcpy(b->ws + b->L.moduli, mf.data(), mf.size() * 4, cudaMemcpyHostToDevice);
     }
+  }
+  if (e == cudaSuccess) {
+    // twiddles of every grid side the batch accepts (the DFT passes read them per plane)
+    if (desc->dtype == TFF_F64)
+      batch_twiddle_kernel<double><<<64, 256>>>(reinterpret_cast<CplxOf<double>::type *>(b->ws + b->L.twiddle),
+                                                kBatchMaxK);
+    else
+      batch_twiddle_kernel<float><<<64, 256>>>(reinterpret_cast<CplxOf<float>::type *>(b->ws + b->L.twiddle),
+                                               kBatchMaxK);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(nullptr);  // the PME streams do not wait for stream 0
   }
   if (e != cudaSuccess) {
     free_batch(b);

@@ -674,9 +674,34 @@ __device__ __forceinline__ int unit_system(const BatchSys *sys, int nsys, int u)
   return lo;
 }
 
-// One plane p of one grid (see batch_dft_kernel).
+// Twiddle table of every grid side 1..kmax: side K at offset K (K - 1) / 2 holds
+// exp(-2 pi i m / K), m = 0..K-1, rounded from FP64. Filled once per batch object.
+__host__ __device__ inline int64_t twiddle_offset(int K) { return (int64_t)K * (K - 1) / 2; }
+
+template <class T>
+__global__ void batch_twiddle_kernel(typename CplxOf<T>::type *tab, int kmax) {
+  const int64_t n = twiddle_offset(kmax + 1);
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    int K = (int)((1.0 + sqrt(1.0 + 8.0 * (double)e)) / 2.0);  // twiddle_offset(K) <= e < twiddle_offset(K + 1)
+    while (twiddle_offset(K) > e) --K;
+    while (twiddle_offset(K + 1) <= e) ++K;
+    const int m = (int)(e - twiddle_offset(K));
+    double sn, cs;
+    sincospi(2.0 * m / K, &sn, &cs);
+    tab[e].x = (T)cs;
+    tab[e].y = (T)(-sn);
+  }
+}
+
+// Lines of a plane each thread transforms at once (one twiddle load serves them all).
+// Measured on a 256-system serving batch (0.85 M atoms): 1 -> 2 -> 4 lines per thread
+// 4.37 -> 4.27 -> 4.25 ms, 8 lines 4.38 ms.
+constexpr int kDftLinesPerThread = 4;
+
+// One plane p of one grid (see batch_dft_kernel); twtab: the batch's twiddle table.
 template <class T, int PASS>
-__device__ __forceinline__ void batch_dft_plane(const BatchSys &b, const int p, T *real, typename CplxOf<T>::type *cplx) {
+__device__ __forceinline__ void batch_dft_plane(const BatchSys &b, const int p, T *real, typename CplxOf<T>::type *cplx,
+                                                const typename CplxOf<T>::type *twtab) {
   using C = typename CplxOf<T>::type;
   const int K = b.K;
   const int Kz = K / 2 + 1, st = dft_stride(K);
@@ -686,10 +711,9 @@ __device__ __forceinline__ void batch_dft_plane(const BatchSys &b, const int p, 
   C *in = tw + K;
   C *out = in + (size_t)K * st;
   for (int m = threadIdx.x; m < K; m += blockDim.x) {
-    double sn, cs;
-    sincospi(2.0 * m / K, &sn, &cs);
-    tw[m].x = (T)cs;
-    tw[m].y = (T)(kInverse ? sn : -sn);
+    C v = twtab[twiddle_offset(K) + m];
+    if (kInverse) v.y = -v.y;
+    tw[m] = v;
   }
   // plane geometry: lines x points in, lines x nout out
   const int lines = (PASS == kDftZR2C || PASS == kDftZC2R) ? K : Kz;
@@ -722,37 +746,68 @@ __device__ __forceinline__ void batch_dft_plane(const BatchSys &b, const int p, 
     in[line * st + pt] = v;
   }
   __syncthreads();
-  // outputs: lane-consecutive lines, one frequency (or z) per output
-  for (int o = threadIdx.x; o < lines * nout; o += blockDim.x) {
-    const int line = o % lines, f = o / lines;
-    const C *row = in + line * st;
-    C acc;
-    acc.x = T(0);
-    acc.y = T(0);
+  // outputs: one frequency (or z) per thread for R lines lg, lg + G, ... (G = ceil(lines / R)):
+  // consecutive lanes take consecutive lines (odd row stride: distinct banks) and each
+  // twiddle load serves R lines. Per output the sum runs over the line in a fixed order.
+  constexpr int R = kDftLinesPerThread;
+  const int G = (lines + R - 1) / R;
+  for (int o = threadIdx.x; o < G * nout; o += blockDim.x) {
+    const int lg = o % G, f = o / G;
+    bool has[R];
+    const C *row[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      has[r] = lg + r * G < lines;
+      row[r] = in + (has[r] ? lg + r * G : lg) * st;
+    }
+    C acc[R];
     if (PASS == kDftZC2R) {
       // real output of a Hermitian half spectrum: T0 + 2 sum_{0<k<K/2} Re(Tk w^(zk)) [+ T_{K/2} (-1)^z]
       const int kh = (K - 1) / 2;
-      T sum = row[0].x;
+      T sum[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) sum[r] = row[r][0].x;
       int idx = 0;
       for (int k = 1; k <= kh; ++k) {
         idx += f;
         if (idx >= K) idx -= K;
-        const C a = row[k], w = tw[idx];
-        sum += T(2) * (a.x * w.x - a.y * w.y);
+        const C w = tw[idx];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const C a = row[r][k];
+          sum[r] += T(2) * (a.x * w.x - a.y * w.y);
+        }
       }
-      if (!(K & 1)) sum += (f & 1) ? -row[K / 2].x : row[K / 2].x;
-      acc.x = sum;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (!(K & 1)) sum[r] += (f & 1) ? -row[r][K / 2].x : row[r][K / 2].x;
+        acc[r].x = sum[r];
+        acc[r].y = T(0);
+      }
     } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) acc[r].x = acc[r].y = T(0);
       int idx = 0;
       for (int j = 0; j < points; ++j) {
-        const C a = row[j], w = tw[idx];
-        acc.x += a.x * w.x - a.y * w.y;
-        acc.y += a.x * w.y + a.y * w.x;
+        const C w = tw[idx];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const C a = row[r][j];
+          if (PASS == kDftZR2C) {  // real input
+            acc[r].x += a.x * w.x;
+            acc[r].y += a.x * w.y;
+          } else {
+            acc[r].x += a.x * w.x - a.y * w.y;
+            acc[r].y += a.x * w.y + a.y * w.x;
+          }
+        }
         idx += f;
         if (idx >= K) idx -= K;
       }
     }
-    out[line * st + f] = acc;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (has[r]) out[(lg + r * G) * st + f] = acc[r];
   }
   __syncthreads();
   // store (global-contiguous order)
@@ -772,11 +827,13 @@ __device__ __forceinline__ void batch_dft_plane(const BatchSys &b, const int p, 
 
 template <class T, int PASS>
 __global__ void __launch_bounds__(kDftThreads) batch_dft_kernel(const BatchSys *sys, const BatchShape *shape, T *real,
-                                                                typename CplxOf<T>::type *cplx, unsigned *counter) {
+                                                                typename CplxOf<T>::type *cplx,
+                                                                const typename CplxOf<T>::type *twtab,
+                                                                unsigned *counter) {
   const int nsys = shape->nsys, units = shape->plane_units;
   for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
     const BatchSys &b = sys[unit_system<true>(sys, nsys, u)];
-    batch_dft_plane<T, PASS>(b, u - b.plane_off, real, cplx);
+    batch_dft_plane<T, PASS>(b, u - b.plane_off, real, cplx, twtab);
   }
 }
 
