@@ -43,9 +43,16 @@ __device__ __forceinline__ void make_stencil(double rx, double ry, double rz, co
     const double m0 = ceil(u);
     const T w = (T)(m0 - u);
     bspline6<T>(w, s.val[d], s.der[d]);
+    // first stencil point modulo K: one compare for atoms within a box length of the
+    // primary cell (the common case), a 64-bit remainder otherwise
     long long g = (long long)m0 - 3;
-    g %= K;
-    if (g < 0) g += K;
+    if (g >= -K && g < 2 * (long long)K) {
+      g += g < 0 ? K : 0;
+      g -= g >= K ? K : 0;
+    } else {
+      g %= K;
+      if (g < 0) g += K;
+    }
     s.g0[d] = (int)g;
   }
 }
@@ -222,8 +229,7 @@ __device__ __forceinline__ void spread_groups(const Atoms &atoms, int64_t n, con
         int mn = 0, mx = 0;
 #pragma unroll
         for (int k = 0; k < kSpreadGroup; ++k) {
-          int v = G[k].org[d] - G[first].org[d];
-          v %= K;
+          int v = G[k].org[d] - G[first].org[d];  // origins lie in [0, K): |v| < K
           if (v > K / 2) v -= K;
           if (v <= -((K + 1) / 2)) v += K;
           rel[k][d] = v;
@@ -251,11 +257,14 @@ __device__ __forceinline__ void spread_groups(const Atoms &atoms, int64_t n, con
             wxy[k] = in ? G[k].q * G[k].w[0][ix] * G[k].w[1][iy] : 0.f;
             oz[k] = in ? rel[k][2] - lo[2] : 1 << 20;  // outside every z
           }
-          int gx = (G[first].org[0] + lo[0] + ax) % K, gy = (G[first].org[1] + lo[1] + ay) % K;
+          // origin in [0, K), lo in (-K/2, 0], ax, ay < 8 <= K: one wrap either way
+          int gx = G[first].org[0] + lo[0] + ax, gy = G[first].org[1] + lo[1] + ay;
           gx += gx < 0 ? K : 0;
+          gx -= gx >= K ? K : 0;
           gy += gy < 0 ? K : 0;
+          gy -= gy >= K ? K : 0;
           const int64_t row = ((int64_t)gx * K + gy) * K;
-          int gz = (G[first].org[2] + lo[2]) % K;
+          int gz = G[first].org[2] + lo[2];
           gz += gz < 0 ? K : 0;
           for (int z = 0; z < ext[2]; ++z) {
             unsigned long long acc = 0ull;
@@ -264,7 +273,7 @@ __device__ __forceinline__ void spread_groups(const Atoms &atoms, int64_t n, con
             for (int k = 0; k < kSpreadGroup; ++k) {
               const int iz = z - oz[k];
               if (iz >= 0 && iz < 6) {
-                acc += to_fix((double)(wxy[k] * G[k].w[2][iz]));
+                acc += to_fix_f(wxy[k] * G[k].w[2][iz]);
                 any = true;
               }
             }
@@ -288,7 +297,7 @@ __device__ __forceinline__ void spread_groups(const Atoms &atoms, int64_t n, con
             const int64_t row = ((int64_t)gx * K + gy) * K;
 #pragma unroll
             for (int c = 0; c < 6; ++c) {
-              atomicAdd(&grid[row + gz], to_fix((double)(wxy * g.w[2][c])));
+              atomicAdd(&grid[row + gz], to_fix_f(wxy * g.w[2][c]));
               gz = (gz + 1 == K) ? 0 : gz + 1;
             }
           }
@@ -338,10 +347,21 @@ __device__ __forceinline__ double convolve_points(typename CplxOf<T>::type *S, c
   const double two_pi = 2.0 * 3.14159265358979323846;
   const double inv4a2 = 1.0 / (4.0 * alpha * alpha);
   double e = 0.0;
+  // 32-bit index arithmetic (a 64-bit division costs several times a 32-bit one) while the
+  // grid has fewer than 2^32 points, i.e. for every K below 2048
+  const bool narrow = total < (int64_t(1) << 32);
   for (int64_t t = bid * blockDim.x + threadIdx.x; t < total; t += nblk * blockDim.x) {
-    const int iz = (int)(t % Kz);
-    const int iy = (int)((t / Kz) % K);
-    const int ix = (int)(t / ((int64_t)Kz * K));
+    int ix, iy, iz;
+    if (narrow) {
+      const unsigned tt = (unsigned)t, row = tt / (unsigned)Kz, x = row / (unsigned)K;
+      iz = (int)(tt - row * (unsigned)Kz);
+      iy = (int)(row - x * (unsigned)K);
+      ix = (int)x;
+    } else {
+      iz = (int)(t % Kz);
+      iy = (int)((t / Kz) % K);
+      ix = (int)(t / ((int64_t)Kz * K));
+    }
     const double mx = (2 * ix < K) ? ix : ix - K;
     const double my = (2 * iy < K) ? iy : iy - K;
     const double mz = (2 * iz < K) ? iz : iz - K;

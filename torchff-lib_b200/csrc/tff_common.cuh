@@ -153,6 +153,11 @@ constexpr double kFixInv = 1.0 / 4294967296.0;
 __device__ __forceinline__ unsigned long long to_fix(double v) {
   return (unsigned long long)__double2ll_rn(v * kFixScale);
 }
+// to_fix of a float without the FP64 steps: v * 2^32 is exact in FP32 as in FP64, so the
+// rounded integer is the same (|v| < 2^31).
+__device__ __forceinline__ unsigned long long to_fix_f(float v) {
+  return (unsigned long long)__float2ll_rn(v * 4294967296.0f);
+}
 __host__ __device__ __forceinline__ double from_fix(unsigned long long v) {
   return (double)(long long)v * kFixInv;
 }
