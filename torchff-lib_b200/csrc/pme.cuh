@@ -430,31 +430,57 @@ struct IndexedGatherOut {
   }
 };
 
-// Gather: kLanesPerAtom lanes per atom as in the spread, partial sums reduced with
-// shuffles inside the lane group (FP64 accumulation of the 216 products). Returns this
-// thread's share of the self energy -(a/sqrt(pi)) sum q^2.
+// Gather: partial sums of the 216 products (FP64 across the stencil rows) reduced with
+// shuffles inside each atom's lane group. Returns this thread's share of the self energy
+// -(a/sqrt(pi)) sum q^2. An atom takes 6 lanes, lane a the x index a of the stencil, so
+// that every other stencil index is a compile-time constant (registers, not local memory);
+// a warp holds 5 atoms (lanes 30, 31 idle). With 8 lanes per atom and the (x, y) row taken
+// from the lane index, the stencil weights went through local memory.
+constexpr int kGatherLanes = 6;
+constexpr int kGatherAtomsPerWarp = kWarp / kGatherLanes;
+
+template <class T>
+__device__ __forceinline__ T pick6(const T (&v)[6], int i) {
+  T r = v[0];
+#pragma unroll
+  for (int k = 1; k < 6; ++k) r = i == k ? v[k] : r;
+  return r;
+}
+
+// Sum over the 6 lanes 6k .. 6k + 5 of an atom, valid on lane 6k (fixed order).
+__device__ __forceinline__ double gather_lane_sum(double v) {
+  v += __shfl_down_sync(kFull, v, 3);
+  const double b1 = __shfl_down_sync(kFull, v, 1), b2 = __shfl_down_sync(kFull, v, 2);
+  return (v + b1) + b2;
+}
+
 template <class T, class Atoms, class Out>
 __device__ __forceinline__ double gather_atoms(const Atoms &atoms, int64_t nthreads, const PmeShared &sh, int K,
                                                const T *Phi, double alpha, const Out &out, int64_t bid,
                                                int64_t nblk) {
   const double a_rpi = alpha / 1.7724538509055160273;
-  const int g = threadIdx.x % kLanesPerAtom;
+  const int lw = threadIdx.x % kWarp;
+  const int slot = lw / kGatherLanes;     // atom of the warp (kGatherAtomsPerWarp: idle lane)
+  const int a = lw - slot * kGatherLanes;  // x index of the stencil
   const int64_t wglob = (bid * blockDim.x + threadIdx.x) / kWarp;
   const int64_t nwarps = nblk * blockDim.x / kWarp;
   double e = 0.0;
-  for (int64_t wb = wglob * kAtomsPerWarp; wb < nthreads; wb += nwarps * kAtomsPerWarp) {
-    const int64_t t = wb + (threadIdx.x % kWarp) / kLanesPerAtom;
+  for (int64_t wb = wglob * kGatherAtomsPerWarp; wb < nthreads; wb += nwarps * kGatherAtomsPerWarp) {
+    const int64_t t = wb + slot;
     double rx = 0.0, ry = 0.0, rz = 0.0;
     T q = T(0);
-    const bool ok = t < nthreads && atoms.get(t, rx, ry, rz, q);
+    const bool ok = slot < kGatherAtomsPerWarp && t < nthreads && atoms.get(t, rx, ry, rz, q);
     double phi = 0.0, du0 = 0.0, du1 = 0.0, du2 = 0.0;
-    Stencil<T> s;
     if (ok) {
+      Stencil<T> s;
       make_stencil<T>(rx, ry, rz, sh.recip, K, s);
-      for (int r = g; r < 36; r += kLanesPerAtom) {
-        const int a = r / 6, b = r % 6;
-        int gx = s.g0[0] + a, gy = s.g0[1] + b;
-        gx -= (gx >= K) ? K : 0;
+      int gx = s.g0[0] + a;
+      gx -= (gx >= K) ? K : 0;
+      // sums over the (y, z) plane at x index a: sum vy pz, sum dy pz, sum vy dz
+      double svp = 0.0, sdp = 0.0, svd = 0.0;
+#pragma unroll
+      for (int b = 0; b < 6; ++b) {
+        int gy = s.g0[1] + b;
         gy -= (gy >= K) ? K : 0;
         const int64_t row = ((int64_t)gx * K + gy) * K;
         int gz = s.g0[2];
@@ -466,21 +492,21 @@ __device__ __forceinline__ double gather_atoms(const Atoms &atoms, int64_t nthre
           dz += v * s.der[2][c];
           gz = (gz + 1 == K) ? 0 : gz + 1;
         }
-        const double vx = (double)s.val[0][a], vy = (double)s.val[1][b];
-        phi += vx * vy * (double)pz;
-        du0 += (double)s.der[0][a] * vy * (double)pz;
-        du1 += vx * (double)s.der[1][b] * (double)pz;
-        du2 += vx * vy * (double)dz;
+        svp += (double)s.val[1][b] * (double)pz;
+        sdp += (double)s.der[1][b] * (double)pz;
+        svd += (double)s.val[1][b] * (double)dz;
       }
+      const double vx = (double)pick6(s.val[0], a), dx = (double)pick6(s.der[0], a);
+      phi = vx * svp;
+      du0 = dx * svp;
+      du1 = vx * sdp;
+      du2 = vx * svd;
     }
-#pragma unroll
-    for (int o = kLanesPerAtom / 2; o > 0; o >>= 1) {
-      phi += __shfl_xor_sync(kFull, phi, o);
-      du0 += __shfl_xor_sync(kFull, du0, o);
-      du1 += __shfl_xor_sync(kFull, du1, o);
-      du2 += __shfl_xor_sync(kFull, du2, o);
-    }
-    if (ok && g == 0) {
+    phi = gather_lane_sum(phi);
+    du0 = gather_lane_sum(du0);
+    du1 = gather_lane_sum(du1);
+    du2 = gather_lane_sum(du2);
+    if (ok && a == 0) {
       // u_d = m0 - frac_d + const, so d(stencil u)/dr_c = -recip[d][c]
       const double qd = (double)q;
       const double gxv = -qd * (du0 * sh.recip[0] + du1 * sh.recip[3] + du2 * sh.recip[6]);
@@ -935,7 +961,7 @@ template <class T>
 // The atoms of a system are visited in the cluster order of the batch's sort (sidx: sorted
 // slot -> batch atom index, -1 for padding), so that neighbouring threads read neighbouring
 // grid points; each atom's numbers are those of the caller-order visit.
-__global__ void __launch_bounds__(kPmeBlock) batch_gather_kernel(const BatchSys *sys, const BatchShape *shape,
+__global__ void __launch_bounds__(kPmeBlock, sizeof(T) == 4 ? 3 : 2) batch_gather_kernel(const BatchSys *sys, const BatchShape *shape,
                                                                  const T *x, const T *q, const int *sidx,
                                                                  const T *boxes, const T *Phi, double alpha, T *phi,
                                                                  T *grad, double *partials, unsigned *tickets,
@@ -1080,7 +1106,7 @@ int pme_gather_phase(const PmePlanImpl &p, const PmeLayout &L, char *ws, Atoms a
   double *partials = reinterpret_cast<double *>(ws + L.partials);
   unsigned *tickets = reinterpret_cast<unsigned *>(ws + L.tickets);
   double *energies = reinterpret_cast<double *>(ws + L.energies);
-  const int64_t lanes = nthreads * kLanesPerAtom;
+  const int64_t lanes = (nthreads + kGatherAtomsPerWarp - 1) / kGatherAtomsPerWarp * kWarp;
   const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((lanes + kPmeBlock - 1) / kPmeBlock, sm_count() * 8));
   pme_gather_kernel<T, Atoms, Out><<<nb, kPmeBlock, 0, s>>>(atoms, nthreads, box, p.K, phi_grid, alpha, out,
                                                             partials, tickets + 1, energies + 1, energies, e_scale,
