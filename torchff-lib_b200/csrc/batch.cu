@@ -43,6 +43,8 @@ inline int moduli_offset(int K) {
 
 // Bytes before the system table in the uploaded block (the BatchShape sits there).
 constexpr size_t kTableOffset = 256;
+// Points of a batched convolution work unit: 8 per thread of a 256-thread block.
+constexpr int64_t kConvPointsPerUnit = 8 * 256;
 static_assert(sizeof(BatchShape) <= kTableOffset, "BatchShape must fit before the system table");
 
 struct BatchLayout {
@@ -179,7 +181,7 @@ int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_g
   auto &hs = b->host_sys;
   hs.assign(nsys, BatchSys{});
   int64_t ao = 0, co = 0, so = 0, go = 0, xo = 0;
-  int pb = 0, planes = 0;
+  int pb = 0, planes = 0, conv = 0;
   for (int i = 0; i < nsys; ++i) {
     const int64_t n = natoms[i];
     const int K = pme_grid[i];
@@ -201,8 +203,13 @@ int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_g
     y.pme_blocks = (int)std::min<int64_t>(kBatchPmeMaxBlocks, std::max<int64_t>(1, (std::max(n * kLanesPerAtom, ncplx) + kPmeBlock - 1) / kPmeBlock));
     y.pb_off = pb;
     y.plane_off = planes;
+    // the convolution's units cover kConvPointsPerUnit points each (its PME blocks, sized
+    // for the atoms, mostly held a few points per thread at most)
+    y.conv_blocks = (int)std::min<int64_t>(kBatchPmeMaxBlocks, std::max<int64_t>(1, (ncplx + kConvPointsPerUnit - 1) / kConvPointsPerUnit));
+    y.conv_off = conv;
     pb += y.pme_blocks;
     planes += K;
+    conv += y.conv_blocks;
     ao += n;
     co += y.ncl;
     so += y.nsup;
@@ -228,6 +235,7 @@ int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_g
   sh.pb_units = pb;
   sh.plane_units = planes;
   sh.kmax = kmax;
+  sh.conv_units = conv;
   // the pinned block is reused once the previous upload out of it is done
   TFF_CUDA(cudaEventSynchronize(b->table_ev));
   std::memcpy(b->table, &sh, sizeof(sh));

@@ -117,6 +117,8 @@ struct BatchSys {
   int pme_blocks;              // blocks of the per-system PME reductions
   int pb_off;                  // the system's first PME work unit (sum of pme_blocks before it)
   int plane_off;               // the system's first DFT plane unit (sum of K before it)
+  int conv_blocks;             // work units (and reduction blocks) of its convolution
+  int conv_off;                // the system's first convolution unit (sum of conv_blocks before it)
   int pad;
 };
 
@@ -129,6 +131,8 @@ struct BatchShape {
   int pb_units;     // PME work units: sum of pme_blocks
   int plane_units;  // DFT plane units: sum of K
   int kmax;
+  int conv_units;   // convolution units: sum of conv_blocks
+  int pad;
 };
 
 // Stride of the per-system box facts (see box_info_kernel).

@@ -705,13 +705,15 @@ __device__ __forceinline__ int next_unit(unsigned *counter) {
 }
 
 // The batch system owning work unit u: the largest s < nsys whose first unit (plane_off for
-// DFT planes, pb_off for PME blocks) is at most u. Every system owns at least one unit.
-template <bool PLANES>
+// DFT planes, pb_off for PME blocks, conv_off for convolution units) is at most u. Every
+// system owns at least one unit of each kind.
+enum BatchUnits { kUnitsPme = 0, kUnitsPlanes, kUnitsConv };
+template <int KIND>
 __device__ __forceinline__ int unit_system(const BatchSys *sys, int nsys, int u) {
   int lo = 0, hi = nsys - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    const int off = PLANES ? sys[mid].plane_off : sys[mid].pb_off;
+    const int off = KIND == kUnitsPlanes ? sys[mid].plane_off : KIND == kUnitsConv ? sys[mid].conv_off : sys[mid].pb_off;
     if (off <= u)
       lo = mid;
     else
@@ -878,7 +880,7 @@ __global__ void __launch_bounds__(kDftThreads) batch_dft_kernel(const BatchSys *
                                                                 unsigned *counter) {
   const int nsys = shape->nsys, units = shape->plane_units;
   for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
-    const BatchSys &b = sys[unit_system<true>(sys, nsys, u)];
+    const BatchSys &b = sys[unit_system<kUnitsPlanes>(sys, nsys, u)];
     batch_dft_plane<T, PASS>(b, u - b.plane_off, real, cplx, twtab);
   }
 }
@@ -928,7 +930,7 @@ __global__ void __launch_bounds__(kPmeBlock, 4) batch_spread_kernel(const BatchS
   __shared__ GroupStencil st[sizeof(T) == 4 ? kPmeBlock / kWarp : 1][kSpreadGroup * kGroupsPerPass];
   const int nsys = shape->nsys, units = shape->pb_units;
   for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
-    const int sy = unit_system<false>(sys, nsys, u);
+    const int sy = unit_system<kUnitsPme>(sys, nsys, u);
     batch_spread_unit<T>(sys, x, q, boxes, grid, sy, u - sys[sy].pb_off, sh,
                          st[sizeof(T) == 4 ? threadIdx.x >> 5 : 0]);
   }
@@ -943,17 +945,17 @@ __global__ void __launch_bounds__(kPmeBlock, 4) batch_convolve_kernel(const Batc
                                                                    unsigned *tickets, double *energies,
                                                                    unsigned *counter) {
   __shared__ PmeShared sh;
-  const int nsys = shape->nsys, units = shape->pb_units;
+  const int nsys = shape->nsys, units = shape->conv_units;
   for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
-    const int sy = unit_system<false>(sys, nsys, u);
+    const int sy = unit_system<kUnitsConv>(sys, nsys, u);
     const BatchSys &b = sys[sy];
-    const int bx = u - b.pb_off;
+    const int bx = u - b.conv_off;
     if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
     __syncthreads();
     const T *xm = moduli + b.mod_off, *ym = xm + b.K, *zm = ym + b.K;
-    const double e = convolve_points<T>(S + b.cplx_off, sh, b.K, alpha, xm, ym, zm, bx, b.pme_blocks);
+    const double e = convolve_points<T>(S + b.cplx_off, sh, b.K, alpha, xm, ym, zm, bx, b.conv_blocks);
     grid_sum_n<kPmeBlock>(0.5 * e, partials + (int64_t)kBatchPmeMaxBlocks * sy, tickets + 2 * sy, energies + 2 * sy,
-                          false, bx, b.pme_blocks);
+                          false, bx, b.conv_blocks);
   }
 }
 
@@ -969,7 +971,7 @@ __global__ void __launch_bounds__(kPmeBlock, sizeof(T) == 4 ? 3 : 2) batch_gathe
   __shared__ PmeShared sh;
   const int nsys = shape->nsys, units = shape->pb_units;
   for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
-    const int sy = unit_system<false>(sys, nsys, u);
+    const int sy = unit_system<kUnitsPme>(sys, nsys, u);
     const BatchSys &b = sys[sy];
     const int bx = u - b.pb_off;
     if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
