@@ -45,6 +45,9 @@ inline int moduli_offset(int K) {
 constexpr size_t kTableOffset = 256;
 // Points of a batched convolution work unit: 8 per thread of a 256-thread block.
 constexpr int64_t kConvPointsPerUnit = 8 * 256;
+// Atoms (sorted slots) of a batched gather work unit: four passes of a 256-thread block at
+// 5 atoms per warp.
+constexpr int64_t kGatherAtomsPerUnit = 4 * (256 / 32) * 5;
 static_assert(sizeof(BatchShape) <= kTableOffset, "BatchShape must fit before the system table");
 
 struct BatchLayout {
@@ -181,7 +184,7 @@ int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_g
   auto &hs = b->host_sys;
   hs.assign(nsys, BatchSys{});
   int64_t ao = 0, co = 0, so = 0, go = 0, xo = 0;
-  int pb = 0, planes = 0, conv = 0;
+  int pb = 0, planes = 0, conv = 0, gat = 0;
   for (int i = 0; i < nsys; ++i) {
     const int64_t n = natoms[i];
     const int K = pme_grid[i];
@@ -207,9 +210,13 @@ int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_g
     // for the atoms, mostly held a few points per thread at most)
     y.conv_blocks = (int)std::min<int64_t>(kBatchPmeMaxBlocks, std::max<int64_t>(1, (ncplx + kConvPointsPerUnit - 1) / kConvPointsPerUnit));
     y.conv_off = conv;
+    // the gather's units take kGatherAtomsPerUnit atoms (the sorted slots of its clusters)
+    y.gather_blocks = (int)std::min<int64_t>(kBatchPmeMaxBlocks, std::max<int64_t>(1, (y.ncl * kWarp + kGatherAtomsPerUnit - 1) / kGatherAtomsPerUnit));
+    y.gather_off = gat;
     pb += y.pme_blocks;
     planes += K;
     conv += y.conv_blocks;
+    gat += y.gather_blocks;
     ao += n;
     co += y.ncl;
     so += y.nsup;
@@ -236,6 +243,7 @@ int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_g
   sh.plane_units = planes;
   sh.kmax = kmax;
   sh.conv_units = conv;
+  sh.gather_units = gat;
   // the pinned block is reused once the previous upload out of it is done
   TFF_CUDA(cudaEventSynchronize(b->table_ev));
   std::memcpy(b->table, &sh, sizeof(sh));

@@ -119,6 +119,8 @@ struct BatchSys {
   int plane_off;               // the system's first DFT plane unit (sum of K before it)
   int conv_blocks;             // work units (and reduction blocks) of its convolution
   int conv_off;                // the system's first convolution unit (sum of conv_blocks before it)
+  int gather_blocks;           // work units (and reduction blocks) of its force gather
+  int gather_off;              // the system's first gather unit
   int pad;
 };
 
@@ -132,7 +134,7 @@ struct BatchShape {
   int plane_units;  // DFT plane units: sum of K
   int kmax;
   int conv_units;   // convolution units: sum of conv_blocks
-  int pad;
+  int gather_units; // gather units: sum of gather_blocks
 };
 
 // Stride of the per-system box facts (see box_info_kernel).

@@ -707,13 +707,16 @@ __device__ __forceinline__ int next_unit(unsigned *counter) {
 // The batch system owning work unit u: the largest s < nsys whose first unit (plane_off for
 // DFT planes, pb_off for PME blocks, conv_off for convolution units) is at most u. Every
 // system owns at least one unit of each kind.
-enum BatchUnits { kUnitsPme = 0, kUnitsPlanes, kUnitsConv };
+enum BatchUnits { kUnitsPme = 0, kUnitsPlanes, kUnitsConv, kUnitsGather };
 template <int KIND>
 __device__ __forceinline__ int unit_system(const BatchSys *sys, int nsys, int u) {
   int lo = 0, hi = nsys - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    const int off = KIND == kUnitsPlanes ? sys[mid].plane_off : KIND == kUnitsConv ? sys[mid].conv_off : sys[mid].pb_off;
+    const int off = KIND == kUnitsPlanes  ? sys[mid].plane_off
+                    : KIND == kUnitsConv  ? sys[mid].conv_off
+                    : KIND == kUnitsGather ? sys[mid].gather_off
+                                           : sys[mid].pb_off;
     if (off <= u)
       lo = mid;
     else
@@ -969,20 +972,20 @@ __global__ void __launch_bounds__(kPmeBlock, sizeof(T) == 4 ? 3 : 2) batch_gathe
                                                                  T *grad, double *partials, unsigned *tickets,
                                                                  double *energies, unsigned *counter) {
   __shared__ PmeShared sh;
-  const int nsys = shape->nsys, units = shape->pb_units;
+  const int nsys = shape->nsys, units = shape->gather_units;
   for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
-    const int sy = unit_system<kUnitsPme>(sys, nsys, u);
+    const int sy = unit_system<kUnitsGather>(sys, nsys, u);
     const BatchSys &b = sys[sy];
-    const int bx = u - b.pb_off;
+    const int bx = u - b.gather_off;
     if (threadIdx.x == 0) load_pme_shared(boxes + 9 * (int64_t)sy, b.K, sh);
     __syncthreads();
     const int *slots = sidx + b.cl_off * kWarp;
     const int64_t nslots = b.ncl * kWarp;
     IndexedAtoms<T> atoms{x, q, slots, nslots};
     IndexedGatherOut<T> out{phi, grad, slots};
-    const double e = gather_atoms<T>(atoms, nslots, sh, b.K, Phi + b.grid_off, alpha, out, bx, b.pme_blocks);
+    const double e = gather_atoms<T>(atoms, nslots, sh, b.K, Phi + b.grid_off, alpha, out, bx, b.gather_blocks);
     grid_sum_n<kPmeBlock>(e, partials + (int64_t)kBatchPmeMaxBlocks * sy, tickets + 2 * sy + 1,
-                          energies + 2 * sy + 1, false, bx, b.pme_blocks);
+                          energies + 2 * sy + 1, false, bx, b.gather_blocks);
   }
 }
 
