@@ -412,3 +412,42 @@ def test_water100k_against_oracle():
     g = O.real_space_grad_subset(wb.coords, wb.box, wb.charges, wb.atom_types, wb.sigma_table, wb.epsilon_table,
                                  wb.coulomb_exclusions, wb.cutoff, wb.alpha, k, subset) + k * g_pme
     assert np.max(np.abs(-f64[subset] - g)) < 1e-8 * np.max(np.abs(g))
+
+
+def _shift_waters(wb, span, seed):
+    """The same box with every water moved by a seeded integer combination of the box
+    vectors (each count in [-span, span]): molecules stay whole, coordinates leave the
+    primary cell by up to `span` box lengths."""
+    import dataclasses
+
+    rng = np.random.default_rng(seed)
+    n = np.rint(rng.uniform(-span, span, (wb.n_waters, 3))).astype(np.float64)
+    shift = np.repeat(n @ wb.box, 3, axis=0)
+    return dataclasses.replace(wb, coords=wb.coords + shift)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_coordinates_outside_the_primary_cell(dtype):
+    """Waters moved by up to 3 box vectors (216 waters; PME stencil origins far outside
+    [0, K) before wrapping): the same energy and forces as the original box. FP64 against
+    the oracle of the original coordinates (energy 1e-10, forces 1e-8 of the largest); mixed
+    precision energy within the usual tolerance and forces within 2e-5 RMS (the coordinates'
+    FP32 rounding at up to 7.5 nm moves atoms by up to 2.4e-7 nm)."""
+    from torchff_b200.system import FixedChargeSystem
+    from torchff_b200.water import water_box_216
+
+    wb = water_box_216()
+    ws = _shift_waters(wb, 3, 5)
+    assert np.abs(ws.coords).max() > 2.5 * wb.box[0, 0]
+    ref = O.fixed_charge_energy(wb.coords, wb.box, wb.charges, wb.sigma_table, wb.epsilon_table, wb.atom_types,
+                                wb.nblist_exclusions, wb.coulomb_exclusions, wb.cutoff, wb.alpha, wb.grid,
+                                138.935456)
+    s = FixedChargeSystem.from_water_box(ws, dtype=dtype)
+    out = s.evaluate(t(ws.coords, dtype), t(ws.box, dtype))
+    assert s.status() == 0
+    if dtype == torch.float64:
+        assert rel(out["energy"].item(), ref["total"]) < 1e-10
+        assert rel_max(out["forces"], -ref["grad_coords"]) < 1e-8
+    else:
+        assert _mixed_energy_err(out["energy"].item(), ref) < 1e-6
+        assert rel_rms(out["forces"], -ref["grad_coords"]) < 2e-5

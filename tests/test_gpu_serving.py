@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 import torch
 
-from gpu_util import rel, rel_max, t
+from gpu_util import rel, rel_max, rel_rms, t
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -274,3 +274,30 @@ def test_graph_replay_serves_other_compositions():
     check("a")                        # the class-52 graph again
     assert ev.graph_launches() == 4
     assert ref_ev.graph_launches() == 0
+
+
+def test_batch_coordinates_outside_the_primary_cell(mixed_boxes):
+    """Batched evaluation of systems whose waters were moved by up to 3 box vectors: energies
+    and forces as for the original coordinates (mixed precision; the coordinates' FP32
+    rounding at a few box lengths bounds the agreement: forces 2e-5 RMS and 1e-4 of the
+    largest, energy 1e-6 of the summed term magnitudes)."""
+    import dataclasses
+
+    from torchff_b200.serving import SystemSpec
+
+    wbs, specs = mixed_boxes
+    moved = []
+    for k, wb in enumerate(wbs[:4]):
+        rng = np.random.default_rng(100 + k)
+        n = np.rint(rng.uniform(-3, 3, (wb.n_waters, 3)))
+        moved.append(dataclasses.replace(wb, coords=wb.coords + np.repeat(n @ wb.box, 3, axis=0)))
+    ev = _evaluator(torch.float32, wbs)
+    e0, f0 = ev.evaluate(specs[:4])
+    e1, f1 = ev.evaluate([SystemSpec.from_water_box(w) for w in moved])
+    torch.cuda.synchronize()
+    assert ev.status() == 0
+    for k, wb in enumerate(wbs[:4]):
+        scale = float(_single(wb, torch.float32)["terms"].abs().sum())
+        assert abs(e1[k].item() - e0[k].item()) < 1e-6 * scale, wb.n_waters
+        assert rel_rms(f1[k], f0[k]) < 2e-5, wb.n_waters
+        assert rel_max(f1[k], f0[k]) < 1e-4, wb.n_waters

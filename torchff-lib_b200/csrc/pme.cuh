@@ -172,7 +172,7 @@ constexpr int kGroupsPerPass = 10;  // most groups staged per warp and pass: 30 
 constexpr int kSpreadWin = 8;
 
 struct GroupStencil {
-  int org[3];    // first stencil point per axis, unwrapped: ceil(u) - 3
+  int org[3];    // first stencil point per axis, ceil(u) - 3 wrapped into [0, K)
   float w[3][6]; // B-spline weights
   float q;
   int valid;
@@ -206,7 +206,17 @@ __device__ __forceinline__ void spread_groups(const Atoms &atoms, int64_t n, con
           const double u = sh.recip[3 * d] * r[0] + sh.recip[3 * d + 1] * r[1] + sh.recip[3 * d + 2] * r[2];
           const double m0 = ceil(u);
           bspline6<float>((float)(m0 - u), g.w[d], der);
-          g.org[d] = (int)m0 - 3;
+          // first stencil point wrapped into [0, K) (the window code below relies on it):
+          // compares within a box length of the primary cell, a 64-bit remainder beyond
+          long long o = (long long)m0 - 3;
+          if (o >= -K && o < 2 * (long long)K) {
+            o += o < 0 ? K : 0;
+            o -= o >= K ? K : 0;
+          } else {
+            o %= K;
+            if (o < 0) o += K;
+          }
+          g.org[d] = (int)o;
         }
         g.q = qa;
       }
@@ -229,7 +239,7 @@ __device__ __forceinline__ void spread_groups(const Atoms &atoms, int64_t n, con
         int mn = 0, mx = 0;
 #pragma unroll
         for (int k = 0; k < kSpreadGroup; ++k) {
-          int v = G[k].org[d] - G[first].org[d];  // origins lie in [0, K): |v| < K
+          int v = G[k].org[d] - G[first].org[d];  // origins lie in [0, K) (wrapped above): |v| < K
           if (v > K / 2) v -= K;
           if (v <= -((K + 1) / 2)) v += K;
           rel[k][d] = v;
