@@ -930,9 +930,9 @@ __device__ __noinline__ void batch_spread_unit(const BatchSys *sys, const T *x, 
   __syncthreads();
   PlainAtoms<T> atoms{x + 3 * b.atom_off, q + b.atom_off, b.natoms};
   if constexpr (sizeof(T) == 4)
-    spread_groups(atoms, b.natoms, sh, b.K, grid + b.grid_off, bx, b.pme_blocks, st);
+    spread_groups(atoms, b.natoms, sh, b.K, grid + b.grid_off, bx, b.gather_blocks, st);
   else
-    spread_atoms<T>(atoms, b.natoms, sh, b.K, grid + b.grid_off, bx, b.pme_blocks);
+    spread_atoms<T>(atoms, b.natoms, sh, b.K, grid + b.grid_off, bx, b.gather_blocks);
 }
 
 template <class T>
@@ -941,10 +941,11 @@ __global__ void __launch_bounds__(kPmeBlock, 4) batch_spread_kernel(const BatchS
                                                                  typename Acc<T>::S *grid, unsigned *counter) {
   __shared__ PmeShared sh;
   __shared__ GroupStencil st[sizeof(T) == 4 ? kPmeBlock / kWarp : 1][kSpreadGroup * kGroupsPerPass];
-  const int nsys = shape->nsys, units = shape->pb_units;
+  // the gather's units (a system's atoms never outnumber its sorted slots)
+  const int nsys = shape->nsys, units = shape->gather_units;
   for (int u = next_unit(counter); u < units; u = next_unit(counter)) {
-    const int sy = unit_system<kUnitsPme>(sys, nsys, u);
-    batch_spread_unit<T>(sys, x, q, boxes, grid, sy, u - sys[sy].pb_off, sh,
+    const int sy = unit_system<kUnitsGather>(sys, nsys, u);
+    batch_spread_unit<T>(sys, x, q, boxes, grid, sy, u - sys[sy].gather_off, sh,
                          st[sizeof(T) == 4 ? threadIdx.x >> 5 : 0]);
   }
 }
