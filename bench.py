@@ -491,7 +491,8 @@ def run_serving(device, n_requests: int = 4096, seed: int = 0) -> dict:
     alpha, rc = boxes[0].alpha, 0.9
     atoms = np.array([s.natoms for s in specs])
     apc, tune_ms = autotune_atoms_per_cell(specs[:64], rc, alpha)
-    lanes, per_batch, budget = 3, 256, 6 << 30
+    # 4 lanes: 3 / 4 / 6 / 8 lanes of 256 systems served 71.4k / 73.6k / 74.3k / 73.3k systems/s
+    lanes, per_batch, budget = 4, 256, 6 << 30
     srv = Server(rc, alpha, torch.float32, lanes=lanes, max_systems_per_batch=per_batch, hbm_budget_bytes=budget,
                  atoms_per_cell=apc, device=device)
 
