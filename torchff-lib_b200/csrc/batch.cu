@@ -184,7 +184,7 @@ int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_g
   auto &hs = b->host_sys;
   hs.assign(nsys, BatchSys{});
   int64_t ao = 0, co = 0, so = 0, go = 0, xo = 0;
-  int pb = 0, planes = 0, conv = 0, gat = 0;
+  int planes = 0, conv = 0, gat = 0;
   for (int i = 0; i < nsys; ++i) {
     const int64_t n = natoms[i];
     const int K = pme_grid[i];
@@ -203,8 +203,6 @@ int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_g
     y.K = K;
     y.mod_off = moduli_offset(K);
     const int64_t ncplx = (int64_t)K * K * (K / 2 + 1);
-    y.pme_blocks = (int)std::min<int64_t>(kBatchPmeMaxBlocks, std::max<int64_t>(1, (std::max(n * kLanesPerAtom, ncplx) + kPmeBlock - 1) / kPmeBlock));
-    y.pb_off = pb;
     y.plane_off = planes;
     // the convolution's units cover kConvPointsPerUnit points each (its PME blocks, sized
     // for the atoms, mostly held a few points per thread at most)
@@ -213,7 +211,6 @@ int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_g
     // the gather's units take kGatherAtomsPerUnit atoms (the sorted slots of its clusters)
     y.gather_blocks = (int)std::min<int64_t>(kBatchPmeMaxBlocks, std::max<int64_t>(1, (y.ncl * kWarp + kGatherAtomsPerUnit - 1) / kGatherAtomsPerUnit));
     y.gather_off = gat;
-    pb += y.pme_blocks;
     planes += K;
     conv += y.conv_blocks;
     gat += y.gather_blocks;
@@ -239,7 +236,6 @@ int batch_prepare(tff_batch b, int nsys, const int64_t *natoms, const int *pme_g
   sh.nsuper = so;
   sh.total_grid = go;
   sh.nsys = nsys;
-  sh.pb_units = pb;
   sh.plane_units = planes;
   sh.kmax = kmax;
   sh.conv_units = conv;

@@ -114,12 +114,10 @@ struct BatchSys {
   int64_t grid_off, cplx_off;  // PME grids: K^3 real points, K*K*(K/2+1) complex points
   int nc, bits;                // cell grid side and Hilbert bits per axis
   int K, mod_off;              // PME grid side and offset of its B-spline moduli
-  int pme_blocks;              // blocks of the per-system PME reductions
-  int pb_off;                  // the system's first PME work unit (sum of pme_blocks before it)
   int plane_off;               // the system's first DFT plane unit (sum of K before it)
   int conv_blocks;             // work units (and reduction blocks) of its convolution
   int conv_off;                // the system's first convolution unit (sum of conv_blocks before it)
-  int gather_blocks;           // work units (and reduction blocks) of its force gather
+  int gather_blocks;           // work units (and reduction blocks) of its force gather; the spread's too
   int gather_off;              // the system's first gather unit
   int pad;
 };
@@ -130,11 +128,11 @@ struct BatchSys {
 struct BatchShape {
   int64_t natoms, nclusters, npad, nsuper, total_grid;
   int nsys;
-  int pb_units;     // PME work units: sum of pme_blocks
   int plane_units;  // DFT plane units: sum of K
   int kmax;
   int conv_units;   // convolution units: sum of conv_blocks
-  int gather_units; // gather units: sum of gather_blocks
+  int gather_units; // gather (and spread) units: sum of gather_blocks
+  int pad;
 };
 
 // Stride of the per-system box facts (see box_info_kernel).

@@ -715,18 +715,17 @@ __device__ __forceinline__ int next_unit(unsigned *counter) {
 }
 
 // The batch system owning work unit u: the largest s < nsys whose first unit (plane_off for
-// DFT planes, pb_off for PME blocks, conv_off for convolution units) is at most u. Every
-// system owns at least one unit of each kind.
-enum BatchUnits { kUnitsPme = 0, kUnitsPlanes, kUnitsConv, kUnitsGather };
+// DFT planes, conv_off for convolution units, gather_off for gather and spread units) is at
+// most u. Every system owns at least one unit of each kind.
+enum BatchUnits { kUnitsPlanes = 0, kUnitsConv, kUnitsGather };
 template <int KIND>
 __device__ __forceinline__ int unit_system(const BatchSys *sys, int nsys, int u) {
   int lo = 0, hi = nsys - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    const int off = KIND == kUnitsPlanes  ? sys[mid].plane_off
-                    : KIND == kUnitsConv  ? sys[mid].conv_off
-                    : KIND == kUnitsGather ? sys[mid].gather_off
-                                           : sys[mid].pb_off;
+    const int off = KIND == kUnitsPlanes ? sys[mid].plane_off
+                    : KIND == kUnitsConv ? sys[mid].conv_off
+                                         : sys[mid].gather_off;
     if (off <= u)
       lo = mid;
     else
@@ -898,11 +897,13 @@ __global__ void __launch_bounds__(kDftThreads) batch_dft_kernel(const BatchSys *
   }
 }
 
-// ---- batched PME: the work units are the PME blocks of every system (system s owns units
-// pb_off .. pb_off + pme_blocks - 1; pme_blocks depends on the system alone, so that its
-// reductions sum in the same order whatever else is in the batch); blocks loop over them.
-// The spread and the convolution keep 4 resident blocks per SM (at most 64 registers): the
-// loop's extra state cost them a block per SM and 29 % / 67 % of their time at 256 systems.
+// ---- batched PME: persistent kernels over work units numbered across the batch. The spread
+// and the gather take units of a system's atoms (system s owns gather_off .. gather_off +
+// gather_blocks - 1), the convolution units of its grid points (conv_off ..); a unit count
+// depends on the system alone, so that its reductions sum in the same order whatever else
+// is in the batch. The spread and the convolution keep 4 resident blocks per SM (at most 64
+// registers): the loop's extra state had cost them a block per SM and 29 % / 67 % of their
+// time at 256 systems.
 constexpr int kBatchPmeMaxBlocks = 256;
 
 // Zeroes the batch's accumulation grid (total_grid points of the shape).
