@@ -317,9 +317,29 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
     T dq[4] = {T(0), T(0), T(0), T(0)};
     double ep = 0.0;
 
+    // J's list entry, position, LJ parameters and slot are loaded one J ahead, so that their
+    // global loads overlap the previous J's arithmetic
+    int Jn = 0, sidn = -1;
+    V pjn{};
+    W2 ljn{};
+    if (ntile > 0) {
+      Jn = cl.nbr[(int64_t)I * cl.cap + k];
+      sidn = cl.sidx[(int64_t)Jn * kWarp + lane];
+      pjn = cl.pos[(int64_t)Jn * kWarp + lane];
+      ljn = A.lj[(int64_t)Jn * kWarp + lane];
+    }
     for (int t = 0; t < ntile; ++t) {
-      const int J = cl.nbr[(int64_t)I * cl.cap + k + t * nch];
+      const int J = Jn;
       const int64_t sJ = (int64_t)J * kWarp;
+      const bool vj = sidn >= 0;
+      V pj = pjn;
+      const W2 lj = ljn;
+      if (t + 1 < ntile) {
+        Jn = cl.nbr[(int64_t)I * cl.cap + k + (t + 1) * nch];
+        sidn = cl.sidx[(int64_t)Jn * kWarp + lane];
+        pjn = cl.pos[(int64_t)Jn * kWarp + lane];
+        ljn = A.lj[(int64_t)Jn * kWarp + lane];
+      }
       // one periodic shift for the whole cluster pair when every pair's displacement then
       // lies within half a box length per axis (orthorhombic boxes)
       bool shifted = false;
@@ -334,8 +354,6 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
         sy = ny * s_m[4];
         sz = nz * s_m[8];
       }
-      const bool vj = cl.sidx[sJ + lane] >= 0;
-      V pj = cl.pos[sJ + lane];
       if (atom_shift) {
         pj.x += rint((cx - pj.x) * s_inv[0]) * s_m[0];
         pj.y += rint((cy - pj.y) * s_inv[4]) * s_m[4];
@@ -353,7 +371,6 @@ __global__ void __launch_bounds__(NW * 32, MIN_BLOCKS) pair_tile_kernel(TileArgs
         pj.w = T(0);
       }
       const unsigned jvalid = __ballot_sync(kFull, vj);
-      const W2 lj = A.lj[sJ + lane];
       __syncwarp();  // every lane is done with the previous J's staging
       {
         // atom lane = 8 cj + tj + 4 h goes to entry 4 cj + tj, slot h of each pair
